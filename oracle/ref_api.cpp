@@ -1,0 +1,424 @@
+// ref_api.cpp -- extern "C" entry points onto the reference's own CPU splat
+// code (test infrastructure).
+//
+// oracle/Makefile compiles this file together with the reference's sources,
+// where they lie (engine/native/cpp/src/splat/{SplatRaster,SplatTrainer,
+// SplatDensify,GaussianCloud}.cpp and src/io/ImageIo.cpp), into
+// oracle/_ref/libpxref_ieee.so (IEEE arithmetic, the parity oracle) and
+// oracle/_ref/libpxref_fast.so (the reference's own -O3 -ffast-math flags,
+// the timed CPU baseline). Nothing here computes anything itself: it only
+// converts between the component-major float arrays of pxs.h and the
+// reference's GaussianCloud / SplatView / SplatGradients types and calls the
+// reference's public functions.
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "parallax/splat/SplatDensify.h"
+#include "parallax/splat/SplatRaster.h"
+#include "parallax/splat/SplatTrainer.h"
+#include "pxs.h"
+
+using namespace parallax;
+
+namespace {
+
+GaussianCloud toCloud(const float* params, int n, int rest, int sh_degree) {
+  GaussianCloud cloud;
+  cloud.sh_degree = sh_degree;
+  cloud.gaussians.resize(static_cast<size_t>(n));
+  const size_t N = static_cast<size_t>(n);
+  for (size_t g = 0; g < N; ++g) {
+    Gaussian& G = cloud.gaussians[g];
+    G.position = Vec3f(params[0 * N + g], params[1 * N + g], params[2 * N + g]);
+    G.log_scale = Vec3f(params[3 * N + g], params[4 * N + g], params[5 * N + g]);
+    G.rotation = Eigen::Quaternionf(params[6 * N + g], params[7 * N + g], params[8 * N + g],
+                                    params[9 * N + g]);
+    G.opacity_logit = params[10 * N + g];
+    for (int c = 0; c < 3; ++c) G.dc[c] = params[(11 + c) * N + g];
+    G.sh_rest.resize(static_cast<size_t>(3 * rest));
+    for (int k = 0; k < 3 * rest; ++k) G.sh_rest[k] = params[(14 + k) * N + g];
+  }
+  return cloud;
+}
+
+int fromCloud(const GaussianCloud& cloud, int rest, float* params, int capacity) {
+  const int n = static_cast<int>(cloud.size());
+  if (n > capacity) return -n;
+  const size_t N = static_cast<size_t>(n);
+  for (size_t g = 0; g < N; ++g) {
+    const Gaussian& G = cloud.gaussians[g];
+    for (int a = 0; a < 3; ++a) {
+      params[(0 + a) * N + g] = G.position[a];
+      params[(3 + a) * N + g] = G.log_scale[a];
+      params[(11 + a) * N + g] = G.dc[a];
+    }
+    params[6 * N + g] = G.rotation.w();
+    params[7 * N + g] = G.rotation.x();
+    params[8 * N + g] = G.rotation.y();
+    params[9 * N + g] = G.rotation.z();
+    params[10 * N + g] = G.opacity_logit;
+    for (int k = 0; k < 3 * rest; ++k) params[(14 + k) * N + g] = G.sh_rest[k];
+  }
+  return n;
+}
+
+SplatView toView(const double* K, int width, int height, const double* R, const double* t) {
+  SplatView view;
+  view.intrinsics.fx = K[0];
+  view.intrinsics.fy = K[1];
+  view.intrinsics.cx = K[2];
+  view.intrinsics.cy = K[3];
+  view.intrinsics.width = width;
+  view.intrinsics.height = height;
+  Mat3 rot;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) rot(r, c) = R[r * 3 + c];
+  view.camera_from_world = Pose(rot, Vec3(t[0], t[1], t[2]));
+  return view;
+}
+
+RasterOptions toOptions(const pxs_raster_options* o) {
+  RasterOptions options;
+  if (o == nullptr) return options;
+  for (int c = 0; c < 3; ++c) options.background[c] = o->background[c];
+  options.sh_degree = o->sh_degree;
+  options.min_alpha = o->min_alpha;
+  options.transmittance_cutoff = o->transmittance_cutoff;
+  options.screen_dilation = o->screen_dilation;
+  return options;
+}
+
+SplatTrainingConfig toConfig(const pxs_train_config* c) {
+  SplatTrainingConfig config;
+  config.iterations = c->iterations;
+  config.position_lr_initial = c->position_lr_initial;
+  config.position_lr_final = c->position_lr_final;
+  config.dc_lr = c->dc_lr;
+  config.sh_rest_lr_divider = c->sh_rest_lr_divider;
+  config.opacity_lr = c->opacity_lr;
+  config.scale_lr = c->scale_lr;
+  config.rotation_lr = c->rotation_lr;
+  config.adam_beta1 = c->adam_beta1;
+  config.adam_beta2 = c->adam_beta2;
+  config.adam_epsilon = c->adam_epsilon;
+  config.ssim_weight = c->ssim_weight;
+  config.sh_degree = c->sh_degree;
+  config.sh_increase_interval = c->sh_increase_interval;
+  config.densify_from_iteration = c->densify_from_iteration;
+  config.densify_until_iteration = c->densify_until_iteration;
+  config.densify_interval = c->densify_interval;
+  config.densify_grad_threshold = c->densify_grad_threshold;
+  config.percent_dense = c->percent_dense;
+  config.split_scale_divider = c->split_scale_divider;
+  config.opacity_reset_interval = c->opacity_reset_interval;
+  config.opacity_reset_value = c->opacity_reset_value;
+  config.prune_opacity = c->prune_opacity;
+  config.prune_scale_fraction = c->prune_scale_fraction;
+  config.max_gaussians = c->max_gaussians;
+  config.seed = c->seed;
+  return config;
+}
+
+void toProjected(const ProjectedSplat& s, pxs_projected_splat* o) {
+  o->index = s.index;
+  o->mean[0] = s.mean.x();
+  o->mean[1] = s.mean.y();
+  for (int i = 0; i < 3; ++i) {
+    o->cov2d[i] = s.cov2d[i];
+    o->conic[i] = s.conic[i];
+    o->color[i] = s.color[i];
+  }
+  o->depth = s.depth;
+  o->radius = s.radius;
+  o->opacity = s.opacity;
+  o->clamped = (s.color_clamped[0] ? 1u : 0u) | (s.color_clamped[1] ? 2u : 0u) |
+               (s.color_clamped[2] ? 4u : 0u);
+}
+
+ProjectedSplat fromProjected(const pxs_projected_splat& o) {
+  ProjectedSplat s;
+  s.index = o.index;
+  s.mean = Vec2f(o.mean[0], o.mean[1]);
+  s.cov2d = Vec3f(o.cov2d[0], o.cov2d[1], o.cov2d[2]);
+  s.conic = Vec3f(o.conic[0], o.conic[1], o.conic[2]);
+  s.depth = o.depth;
+  s.radius = o.radius;
+  for (int i = 0; i < 3; ++i) {
+    s.color[i] = o.color[i];
+    s.color_clamped[i] = (o.clamped >> i) & 1u;
+  }
+  s.opacity = o.opacity;
+  return s;
+}
+
+void addGradients(const SplatGradients& g, int rest, float* grads, float* screen, int32_t* visible) {
+  const size_t N = g.position.size();
+  for (size_t i = 0; i < N; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      grads[(0 + a) * N + i] += g.position[i][a];
+      grads[(3 + a) * N + i] += g.log_scale[i][a];
+      grads[(11 + a) * N + i] += g.dc[i][a];
+    }
+    for (int a = 0; a < 4; ++a) grads[(6 + a) * N + i] += g.rotation[i][a];
+    grads[10 * N + i] += g.opacity_logit[i];
+    for (int k = 0; k < 3 * rest; ++k)
+      grads[(14 + k) * N + i] += g.sh_rest[i * static_cast<size_t>(3 * rest) + k];
+    screen[i] += g.screen_gradient[i];
+    visible[i] += g.visible_count[i];
+  }
+}
+
+struct RefTrainer {
+  std::unique_ptr<SplatTrainer> trainer;
+  int rest = 0;
+};
+
+}  // namespace
+
+extern "C" {
+
+void ref_camera(const double* K, int width, int height, const double* R, const double* t,
+                pxs_camera* out) {
+  // The float values projectSplats derives from a SplatView (SplatRaster.cpp:206-212).
+  const SplatView view = toView(K, width, height, R, t);
+  const Eigen::Matrix3f W = view.camera_from_world.R.cast<float>();
+  const Vec3f tf = view.camera_from_world.t.cast<float>();
+  const Vec3f center = view.camera_from_world.center().cast<float>();
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out->R[r * 3 + c] = W(r, c);
+  for (int i = 0; i < 3; ++i) {
+    out->t[i] = tf[i];
+    out->center[i] = center[i];
+  }
+  const CameraIntrinsics& k = view.intrinsics;
+  out->fx = static_cast<float>(k.fx);
+  out->fy = static_cast<float>(k.fy);
+  out->cx = static_cast<float>(k.cx);
+  out->cy = static_cast<float>(k.cy);
+  out->tan_half_x = static_cast<float>(0.5 * k.width / k.fx);
+  out->tan_half_y = static_cast<float>(0.5 * k.height / k.fy);
+  out->width = width;
+  out->height = height;
+}
+
+int ref_project(const float* params, int n, int rest, int cloud_sh, const double* K, int width,
+                int height, const double* R, const double* t, const pxs_raster_options* opt,
+                pxs_projected_splat* out) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const std::vector<ProjectedSplat> p =
+      projectSplats(cloud, toView(K, width, height, R, t), toOptions(opt));
+  for (size_t i = 0; i < p.size(); ++i) toProjected(p[i], &out[i]);
+  return static_cast<int>(p.size());
+}
+
+void ref_rasterize(const pxs_projected_splat* projected, int count, const double* K, int width,
+                   int height, const double* R, const double* t, const pxs_raster_options* opt,
+                   float* rgb, float* transmittance) {
+  std::vector<ProjectedSplat> p;
+  p.reserve(static_cast<size_t>(count));
+  for (int i = 0; i < count; ++i) p.push_back(fromProjected(projected[i]));
+  const SplatImage image = rasterizeSplats(p, toView(K, width, height, R, t), toOptions(opt));
+  std::memcpy(rgb, image.rgb.data(), image.rgb.size() * sizeof(float));
+  if (transmittance != nullptr) {
+    std::memcpy(transmittance, image.transmittance.data(),
+                image.transmittance.size() * sizeof(float));
+  }
+}
+
+void ref_render(const float* params, int n, int rest, int cloud_sh, const double* K, int width,
+                int height, const double* R, const double* t, const pxs_raster_options* opt,
+                float* rgb, float* transmittance) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const SplatImage image =
+      renderSplats(cloud, toView(K, width, height, R, t), toOptions(opt));
+  std::memcpy(rgb, image.rgb.data(), image.rgb.size() * sizeof(float));
+  if (transmittance != nullptr) {
+    std::memcpy(transmittance, image.transmittance.data(),
+                image.transmittance.size() * sizeof(float));
+  }
+}
+
+float ref_photometric_loss(const float* rendered, const float* target, int width, int height,
+                           float ssim_weight, float* dL_drgb) {
+  SplatImage image;
+  image.width = width;
+  image.height = height;
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  image.rgb.assign(rendered, rendered + values);
+  image.transmittance.assign(values / 3, 0.f);
+  std::vector<float> tgt(target, target + values);
+  std::vector<float> grad;
+  const float loss = photometricLoss(image, tgt, ssim_weight, dL_drgb ? &grad : nullptr);
+  if (dL_drgb != nullptr) std::memcpy(dL_drgb, grad.data(), values * sizeof(float));
+  return loss;
+}
+
+float ref_mean_ssim(const float* rendered, const float* target, int width, int height,
+                    float* d_rendered) {
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  std::vector<float> a(rendered, rendered + values), b(target, target + values), d;
+  const float ssim = meanSsim(a, b, width, height, d_rendered ? &d : nullptr);
+  if (d_rendered != nullptr) std::memcpy(d_rendered, d.data(), values * sizeof(float));
+  return ssim;
+}
+
+// rasterizeSplatsBackward after the reference's own projection and forward.
+void ref_backward(const float* params, int n, int rest, int cloud_sh, const double* K,
+                  int width, int height, const double* R, const double* t,
+                  const pxs_raster_options* opt, const float* dL_drgb, float* grads,
+                  float* screen, int32_t* visible) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const SplatView view = toView(K, width, height, R, t);
+  const RasterOptions options = toOptions(opt);
+  const std::vector<ProjectedSplat> p = projectSplats(cloud, view, options);
+  const SplatImage image = rasterizeSplats(p, view, options);
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  std::vector<float> dL(dL_drgb, dL_drgb + values);
+  SplatGradients g;
+  g.resize(cloud.size(), 3 * rest);
+  rasterizeSplatsBackward(cloud, view, options, p, image, dL, &g);
+  addGradients(g, rest, grads, screen, visible);
+}
+
+// CpuSplatBackend::renderAndAccumulate (SplatTrainer.cpp:104-113).
+float ref_render_and_accumulate(const float* params, int n, int rest, int cloud_sh,
+                                const double* K, int width, int height, const double* R,
+                                const double* t, const pxs_raster_options* opt,
+                                const float* target, float ssim_weight, float* grads,
+                                float* screen, int32_t* visible) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const SplatView view = toView(K, width, height, R, t);
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  std::vector<float> tgt(target, target + values);
+  SplatGradients g;
+  g.resize(cloud.size(), 3 * rest);
+  std::unique_ptr<SplatBackend> backend = makeCpuSplatBackend();
+  const float loss =
+      backend->renderAndAccumulate(cloud, view, toOptions(opt), tgt, ssim_weight, &g);
+  addGradients(g, rest, grads, screen, visible);
+  return loss;
+}
+
+// densifyAndPrune (SplatDensify.cpp:28-109). `params` has room for
+// config->max_gaussians gaussians; output stride is the new count.
+int ref_densify(float* params, int n, int rest, const float* screen, const int32_t* visible,
+                const pxs_train_config* config, float extent, int iteration, uint32_t* rng,
+                int32_t* source, int32_t* cloned, int32_t* split, int32_t* pruned) {
+  GaussianCloud cloud = toCloud(params, n, rest, 3);
+  SplatDensifyStats stats;
+  stats.screen_gradient.assign(screen, screen + n);
+  stats.visible_count.assign(visible, visible + n);
+  const SplatDensifyResult r =
+      densifyAndPrune(&cloud, stats, toConfig(config), extent, iteration, rng);
+  for (size_t i = 0; i < r.source_index.size(); ++i) source[i] = r.source_index[i];
+  *cloned = r.cloned;
+  *split = r.split;
+  *pruned = r.pruned;
+  return fromCloud(cloud, rest, params, config->max_gaussians);
+}
+
+// ------------------------------------------------------------- the trainer
+
+void* ref_trainer_create(const float* params, int n, int rest, int cloud_sh, int n_views,
+                         const double* K, const int32_t* sizes, const double* R,
+                         const double* t, const float* const* images,
+                         const pxs_train_config* config) {
+  std::vector<SplatTrainingView> views;
+  for (int v = 0; v < n_views; ++v) {
+    SplatTrainingView tv;
+    tv.view = toView(K + 4 * v, sizes[2 * v], sizes[2 * v + 1], R + 9 * v, t + 3 * v);
+    const size_t values = static_cast<size_t>(sizes[2 * v]) * sizes[2 * v + 1] * 3;
+    tv.image.assign(images[v], images[v] + values);
+    views.push_back(std::move(tv));
+  }
+  auto* holder = new RefTrainer;
+  holder->rest = rest;
+  holder->trainer = std::make_unique<SplatTrainer>(toCloud(params, n, rest, cloud_sh),
+                                                   std::move(views), toConfig(config));
+  return holder;
+}
+
+void ref_trainer_destroy(void* handle) { delete static_cast<RefTrainer*>(handle); }
+
+int ref_trainer_step(void* handle) { return static_cast<RefTrainer*>(handle)->trainer->step(); }
+
+// Runs SplatTrainer::train with a callback that cancels once `cancel_at` is
+// reached (0 never cancels). Returns train()'s result; `seen` gets the last
+// iteration the callback saw.
+int ref_trainer_train(void* handle, int cancel_at, int* seen) {
+  int last = 0;
+  const bool done =
+      static_cast<RefTrainer*>(handle)->trainer->train([&](const SplatTrainingProgress& p) {
+        last = p.iteration;
+        return cancel_at <= 0 || p.iteration < cancel_at;
+      });
+  if (seen != nullptr) *seen = last;
+  return done ? 1 : 0;
+}
+
+void ref_trainer_state(void* handle, int* iteration, int* count, float* last_loss,
+                       float* smoothed, float* extent, int* sh_degree) {
+  const SplatTrainer& tr = *static_cast<RefTrainer*>(handle)->trainer;
+  *iteration = tr.iteration();
+  *count = static_cast<int>(tr.cloud().size());
+  *last_loss = tr.lastLoss();
+  *smoothed = tr.smoothedLoss();
+  *extent = tr.sceneExtent();
+  *sh_degree = tr.shDegreeInUse();
+}
+
+int ref_trainer_download(void* handle, float* params, int capacity) {
+  auto* h = static_cast<RefTrainer*>(handle);
+  return fromCloud(h->trainer->cloud(), h->rest, params, capacity);
+}
+
+int ref_trainer_finish(void* handle, float* params, int capacity, int* sh_degree) {
+  auto* h = static_cast<RefTrainer*>(handle);
+  const GaussianCloud cloud = h->trainer->finish();
+  if (sh_degree != nullptr) *sh_degree = cloud.sh_degree;
+  return fromCloud(cloud, h->rest, params, capacity);
+}
+
+int ref_config_validate(const pxs_train_config* config, char* reason, int len) {
+  const std::string why = toConfig(config).validate();
+  if (reason != nullptr && len > 0) {
+    std::strncpy(reason, why.c_str(), static_cast<size_t>(len) - 1);
+    reason[len - 1] = '\0';
+  }
+  return why.empty() ? 0 : 1;
+}
+
+void ref_config_defaults(pxs_train_config* c) {
+  const SplatTrainingConfig d;
+  c->iterations = d.iterations;
+  c->position_lr_initial = d.position_lr_initial;
+  c->position_lr_final = d.position_lr_final;
+  c->dc_lr = d.dc_lr;
+  c->sh_rest_lr_divider = d.sh_rest_lr_divider;
+  c->opacity_lr = d.opacity_lr;
+  c->scale_lr = d.scale_lr;
+  c->rotation_lr = d.rotation_lr;
+  c->adam_beta1 = d.adam_beta1;
+  c->adam_beta2 = d.adam_beta2;
+  c->adam_epsilon = d.adam_epsilon;
+  c->ssim_weight = d.ssim_weight;
+  c->sh_degree = d.sh_degree;
+  c->sh_increase_interval = d.sh_increase_interval;
+  c->densify_from_iteration = d.densify_from_iteration;
+  c->densify_until_iteration = d.densify_until_iteration;
+  c->densify_interval = d.densify_interval;
+  c->densify_grad_threshold = d.densify_grad_threshold;
+  c->percent_dense = d.percent_dense;
+  c->split_scale_divider = d.split_scale_divider;
+  c->opacity_reset_interval = d.opacity_reset_interval;
+  c->opacity_reset_value = d.opacity_reset_value;
+  c->prune_opacity = d.prune_opacity;
+  c->prune_scale_fraction = d.prune_scale_fraction;
+  c->max_gaussians = d.max_gaussians;
+  c->seed = d.seed;
+}
+
+}  // extern "C"
