@@ -288,6 +288,40 @@ int pxs_trainer_step_batch(pxs_trainer* trainer, int32_t n_views, const int32_t*
 int pxs_trainer_step_views(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                            float* loss);
 
+/* Renders the trainer's current cloud from `camera` into host memory (rgb
+ * width*height*3, transmittance width*height or NULL): SplatBackend::render
+ * (SplatTrainer.h:123-124). NULL options use the trainer's current ones. */
+int pxs_trainer_render(pxs_trainer* trainer, const pxs_camera* camera,
+                       const pxs_raster_options* options, float* rgb, float* transmittance);
+
+/* Measures this device's FP32 FMA throughput (TFLOP/s) with a microkernel:
+ * the roofline denominator of the FP32-bound compositing kernels. */
+int pxs_measure_fp32_peak(int32_t device, float* tflops);
+
+/* The CUDA stream (a cudaStream_t) the trainer's kernels run on. */
+int pxs_trainer_stream(pxs_trainer* trainer, void** stream);
+
+/* Stage timing of the batched step: when enabled, CUDA events are recorded on
+ * the trainer's stream between its stages (project, bin, forward, loss,
+ * backward, param_grads, adam; inside the captured graph as event nodes) and
+ * their elapsed times accumulated. pxs_trainer_stage_times returns the
+ * accumulated milliseconds per stage and the number of steps timed. */
+int pxs_trainer_set_timing(pxs_trainer* trainer, int32_t enable);
+int pxs_trainer_stage_times(pxs_trainer* trainer, float* ms, int32_t capacity,
+                            int32_t* n_stages, int32_t* n_steps);
+
+/* Tile pairs and kernel launches of the last step. */
+int pxs_trainer_step_info(pxs_trainer* trainer, int64_t* pairs, int64_t* kernel_launches);
+
+/* Re-runs the last batch's forward pass counting the (pixel, entry) pairs the
+ * compositing loop evaluates and those passing both alpha tests. */
+int pxs_trainer_pair_stats(pxs_trainer* trainer, int64_t* evaluated, int64_t* contributing);
+
+/* Replaces the resident target images of `view_ids` from host memory (queued
+ * on the trainer's stream; pinned memory makes the copies asynchronous). */
+int pxs_trainer_set_images(pxs_trainer* trainer, int32_t n, const int32_t* view_ids,
+                           const float* const* images);
+
 /* iteration, gaussian count, last loss, smoothed loss, scene extent and the
  * SH degree in use (SplatTrainer.h:144-153). Any pointer may be NULL. */
 int pxs_trainer_state(pxs_trainer* trainer, int32_t* iteration, int32_t* count,

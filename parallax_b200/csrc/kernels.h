@@ -1,0 +1,103 @@
+// kernels.h -- host-side launchers of the sm_100a kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pxs {
+
+// Per-step optimiser scalars, read by the Adam kernel from device memory so a
+// captured graph picks up each step's values.
+struct StepScalars {
+  float lr[6];  // position, log_scale, rotation, opacity, dc, sh_rest
+  float beta1, beta2, epsilon;
+  float correction1, correction2;
+  float pad;
+};
+
+struct LossParams {
+  float kernel[11];   // ssimKernel() (SplatRaster.cpp:587-600), computed on the host
+  float ssim_weight;
+  int mode;           // 0 photometric loss gradient, 1 SSIM gradient
+};
+
+struct ScanScratch {
+  static constexpr int kLevels = 6;
+  char* level[kLevels] = {};
+};
+
+// project.cu
+void launch_project(const float* params, int N, int S, int64_t slot_stride,
+                    const ViewDesc* views, int n_views, const ProjectedSoA& out,
+                    cudaStream_t stream);
+void launch_param_grads(const float* params, int N, int S, int64_t slot_stride,
+                        const ViewDesc* views, int n_views, const uint32_t* depth_key,
+                        const float4* conic_op, const float4* color, const ScreenGrad* screen,
+                        float* grads, float* screen_gradient, int32_t* visible_count,
+                        cudaStream_t stream);
+
+// sort.cu
+size_t scan_scratch_bytes(int64_t n, int level = 0);
+void scan_scratch_assign(ScanScratch& s, char* base, int64_t n);
+void exclusive_scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* total,
+                               ScanScratch& scratch, cudaStream_t stream);
+void exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, ScanScratch& scratch,
+                        cudaStream_t stream);
+size_t radix_hist_entries(int64_t n, int64_t segment_len, int max_bits);
+// Sorts (keys, vals) by the low `total_bits` bits of the keys, stably, each
+// `segment_len` run independently (segment_len a multiple of kSortTile, or 0
+// for one segment). keys/vals and the *_alt buffers are swapped so that on
+// return keys/vals hold the result. Returns the number of passes.
+int radix_sort_pairs(uint32_t*& keys, uint32_t*& vals, uint32_t*& keys_alt,
+                     uint32_t*& vals_alt, int64_t n, int64_t segment_len, int total_bits,
+                     uint32_t* hist, uint32_t* hist_scanned, ScanScratch& scratch,
+                     cudaStream_t stream, const int64_t* n_device = nullptr);
+void launch_iota(uint32_t* out, int64_t n, cudaStream_t stream);
+void launch_gather_counts(const uint32_t* sorted_slots, const int32_t* tile_count, int64_t n,
+                          int32_t* counts, cudaStream_t stream);
+void launch_emit_pairs(const uint32_t* sorted_slots, const int32_t* counts,
+                       const int64_t* offsets, const uint2* rect, const ViewDesc* views,
+                       int64_t slot_stride, int64_t n, uint32_t* keys, uint32_t* vals,
+                       int64_t capacity, uint32_t sentinel_tile, int32_t* overflow,
+                       cudaStream_t stream);
+// n is an upper bound when n_device (the device-side pair count) is given.
+void launch_tile_ranges(const uint32_t* keys, int64_t n, const int64_t* n_device,
+                        uint32_t n_tiles, int2* ranges, cudaStream_t stream);
+
+// raster.cu
+void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                    const float4* conic_op, const float4* color, const ViewDesc* views,
+                    int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
+                    cudaStream_t stream, unsigned long long* counts = nullptr);
+void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                     const float4* conic_op, const float4* color, const ViewDesc* views,
+                     int n_views, int total_tiles, const float* T_final, const int32_t* last,
+                     const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream);
+
+// loss.cu
+size_t loss_smem_bytes();
+void configure_loss_kernel();  // once per device, outside graph capture
+void launch_loss(const float* rendered, const float* target, const ViewDesc* views, int n_views,
+                 int max_width, int max_height, const LossParams& lp, float* grad_out,
+                 double* sums, float* per_view, float* total, cudaStream_t stream);
+
+// peak.cu
+float measure_fp32_peak_tflops(cudaStream_t stream);
+
+// adam.cu
+void launch_adam(float* params, float* grads, float* m, float* v, int N, int S,
+                 const StepScalars* scalars, int zero_grads, float* screen_gradient,
+                 int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
+                 cudaStream_t stream);
+// Same step, skipped entirely when *skip is nonzero (a batch whose pairs overflowed).
+void launch_adam_checked(float* params, float* grads, float* m, float* v, int N, int S,
+                         const StepScalars* scalars, float* screen_gradient,
+                         int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
+                         const int32_t* skip, cudaStream_t stream);
+void launch_reset_opacity(float* params, float* m, float* v, int N, float ceiling,
+                          cudaStream_t stream);
+
+}  // namespace pxs

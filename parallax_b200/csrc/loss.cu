@@ -1,0 +1,252 @@
+// loss.cu -- photometric loss L = (1-w) mean|r-t| + w (1 - mean SSIM) and its
+// gradient, fused into one shared-memory tiled kernel.
+//
+// photometricLoss / meanSsim (SplatRaster.cpp:582-738) run 13 separable
+// blurs per channel over whole-image planes. Here a CTA owns a 32x16 output
+// tile and stages the rendered and target images over a 10-pixel halo (two
+// stacked 11-tap blurs): it blurs the five statistic planes (x, y, xx, yy, xy)
+// onto a 5-pixel halo, forms the SSIM map and its three partials there
+// (zero outside the image, as the reference's zero-padded adjoint requires),
+// blurs the five partial planes back onto the tile and writes dL/drgb.
+// Sums run in the reference's tap order and the file is compiled with
+// -fmad=false, so each per-pixel value rounds as the reference's does; the
+// scalar totals are accumulated in double.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pxs {
+namespace {
+
+constexpr int TW = 32, TH = 16;
+constexpr int IW = TW + 20, IH = TH + 20;  // input region
+constexpr int SW = TW + 10, SH = TH + 10;  // statistics region
+constexpr int kThreads = 256;
+
+struct LossSmem {
+  float in_r[3][IH][IW];   // rendered, all channels
+  float in_t[3][IH][IW];   // target
+  float hb[5][IH][SW];     // horizontal blur of the five products / of the partials
+  float st[5][SH][SW];     // statistics, then in place the five partial planes
+};
+
+}  // namespace
+
+// mode 0: dL/drgb of photometricLoss; mode 1: d(mean SSIM)/drgb (meanSsim).
+__global__ void __launch_bounds__(kThreads)
+    k_loss(const float* __restrict__ rendered, const float* __restrict__ target,
+           const ViewDesc* __restrict__ views, int n_views, LossParams lp,
+           float* __restrict__ grad_out, double* __restrict__ sums) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LossSmem& sm = *reinterpret_cast<LossSmem*>(smem_raw);
+  const int v = blockIdx.z;
+  const ViewDesc& vd = views[v];
+  const int W = vd.cam.width, H = vd.cam.height;
+  const int ox = blockIdx.x * TW, oy = blockIdx.y * TH;
+  if (ox >= W || oy >= H) return;
+  const int64_t pix0 = vd.pixel_offset;
+  const float* rimg = rendered + pix0 * 3;
+  const float* timg = target + vd.target_offset * 3;
+  const int tid = threadIdx.x;
+
+  // stage both images over the input region, zero outside
+  for (int i = tid; i < IH * IW * 3; i += kThreads) {
+    const int c = i % 3;
+    const int q = i / 3;
+    const int lx = q % IW, ly = q / IW;
+    const int X = ox - 10 + lx, Y = oy - 10 + ly;
+    float a = 0.f, b = 0.f;
+    if (X >= 0 && X < W && Y >= 0 && Y < H) {
+      const int64_t o = ((int64_t)Y * W + X) * 3 + c;
+      a = rimg[o];
+      b = timg[o];
+    }
+    sm.in_r[c][ly][lx] = a;
+    sm.in_t[c][ly][lx] = b;
+  }
+  __syncthreads();
+
+  const float w = lp.ssim_weight;
+  // 1 / values and 1 / (pixels * 3) of photometricLoss and meanSsim: equal
+  const float inv = 1.f / (float)((int64_t)W * H * 3);
+  const float scale = inv;
+  const float c1 = 0.01f * 0.01f, c2 = 0.03f * 0.03f;
+  double l1_sum = 0.0, ssim_sum = 0.0;
+  const bool want_ssim = lp.mode == 1 || w > 0.f;
+
+  for (int c = 0; c < 3; ++c) {
+    if (want_ssim) {
+      // horizontal blur of the five products, every input row, stats columns
+      for (int i = tid; i < IH * SW; i += kThreads) {
+        const int r = i / SW, col = i % SW;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          const float x = sm.in_r[c][r][col + k], y = sm.in_t[c][r][col + k];
+          const float kk = lp.kernel[k];
+          s0 += kk * x;
+          s1 += kk * y;
+          s2 += kk * (x * x);
+          s3 += kk * (y * y);
+          s4 += kk * (x * y);
+        }
+        sm.hb[0][r][col] = s0;
+        sm.hb[1][r][col] = s1;
+        sm.hb[2][r][col] = s2;
+        sm.hb[3][r][col] = s3;
+        sm.hb[4][r][col] = s4;
+      }
+      __syncthreads();
+      // vertical blur -> statistics, then the SSIM map and its partials in place
+      for (int i = tid; i < SH * SW; i += kThreads) {
+        const int r = i / SW, col = i % SW;
+        float m[5];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+          float s = 0.f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.hb[p][r + k][col];
+          m[p] = s;
+        }
+        const int X = ox - 5 + col, Y = oy - 5 + r;
+        float t_mu = 0.f, t_var = 0.f, t_cov = 0.f, mu_x = m[0], mu_y = m[1];
+        if (X >= 0 && X < W && Y >= 0 && Y < H) {
+          const float var_x = m[2] - mu_x * mu_x;
+          const float var_y = m[3] - mu_y * mu_y;
+          const float cov = m[4] - mu_x * mu_y;
+          const float a = 2.f * mu_x * mu_y + c1;
+          const float b = 2.f * cov + c2;
+          const float cc = mu_x * mu_x + mu_y * mu_y + c1;
+          const float d = var_x + var_y + c2;
+          if (col >= 5 && col < 5 + TW && r >= 5 && r < 5 + TH) ssim_sum += (double)((a * b) / (cc * d));
+          t_mu = scale * (2.f * mu_y * b / (cc * d) - 2.f * mu_x * a * b / (cc * cc * d));
+          t_var = scale * (-(a * b) / (cc * d * d));
+          t_cov = scale * (2.f * a / (cc * d));
+        } else {
+          mu_x = 0.f;
+          mu_y = 0.f;
+        }
+        sm.st[0][r][col] = t_mu;
+        sm.st[1][r][col] = t_var;
+        sm.st[2][r][col] = t_var * mu_x;
+        sm.st[3][r][col] = t_cov;
+        sm.st[4][r][col] = t_cov * mu_y;
+      }
+      __syncthreads();
+      // horizontal blur of the partials onto the tile's columns
+      for (int i = tid; i < SH * TW; i += kThreads) {
+        const int r = i / TW, col = i % TW;
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+          float s = 0.f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.st[p][r][col + k];
+          sm.hb[p][r][col] = s;
+        }
+      }
+      __syncthreads();
+    }
+    // vertical blur and the gradient at each tile pixel
+    for (int i = tid; i < TH * TW; i += kThreads) {
+      const int r = i / TW, col = i % TW;
+      const int X = ox + col, Y = oy + r;
+      if (X >= W || Y >= H) continue;
+      const float x = sm.in_r[c][r + 10][col + 10];
+      const float y = sm.in_t[c][r + 10][col + 10];
+      float d = 0.f;
+      if (want_ssim) {
+        float B[5];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+          float s = 0.f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.hb[p][r + k][col];
+          B[p] = s;
+        }
+        d = 0.f + B[0];
+        d += 2.f * x * B[1];
+        d -= 2.f * B[2];
+        d += y * B[3];
+        d -= B[4];
+      }
+      const int64_t o = (pix0 + (int64_t)Y * W + X) * 3 + c;
+      if (lp.mode == 1) {
+        grad_out[o] = d;
+      } else {
+        const float diff = x - y;
+        l1_sum += (double)fabsf(diff);
+        const float sign = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
+        float g = (1.f - w) * sign * inv;
+        if (w > 0.f) g -= w * d;
+        if (grad_out != nullptr) grad_out[o] = g;
+      }
+    }
+    __syncthreads();
+  }
+  // block sums -> per-view totals
+  __shared__ double red[2][kThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    l1_sum += __shfl_xor_sync(0xffffffffu, l1_sum, o);
+    ssim_sum += __shfl_xor_sync(0xffffffffu, ssim_sum, o);
+  }
+  if (lane_id() == 0) {
+    red[0][warp_id()] = l1_sum;
+    red[1][warp_id()] = ssim_sum;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < kThreads / 32; ++k) {
+      a += red[0][k];
+      b += red[1][k];
+    }
+    atomicAdd(&sums[2 * v + 0], a);
+    atomicAdd(&sums[2 * v + 1], b);
+  }
+}
+
+// loss = (1-w) * l1 + w * (1 - ssim) per view (SplatRaster.cpp:737); the
+// batch loss is the mean over views. mode 1 reports mean SSIM instead.
+__global__ void k_loss_finalize(const double* __restrict__ sums, const ViewDesc* views,
+                                int n_views, float ssim_weight, int mode,
+                                float* __restrict__ per_view, float* __restrict__ total) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float sum = 0.f;
+  for (int v = 0; v < n_views; ++v) {
+    const double values = 3.0 * (double)views[v].cam.width * (double)views[v].cam.height;
+    float loss;
+    const float ssim = (float)(sums[2 * v + 1] / values);
+    if (mode == 1) {
+      loss = ssim;
+    } else {
+      const float l1 = (float)(sums[2 * v + 0] / values);
+      loss = ssim_weight <= 0.f ? l1 : (1.f - ssim_weight) * l1 + ssim_weight * (1.f - ssim);
+    }
+    if (per_view != nullptr) per_view[v] = loss;
+    sum += loss;
+  }
+  if (total != nullptr) *total = n_views > 0 ? sum / (float)n_views : 0.f;
+}
+
+size_t loss_smem_bytes() { return sizeof(LossSmem); }
+
+void configure_loss_kernel() {
+  cudaFuncSetAttribute(k_loss, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LossSmem));
+}
+
+void launch_loss(const float* rendered, const float* target, const ViewDesc* views, int n_views,
+                 int max_width, int max_height, const LossParams& lp, float* grad_out,
+                 double* sums, float* per_view, float* total, cudaStream_t stream) {
+  if (n_views <= 0) return;
+  cudaMemsetAsync(sums, 0, sizeof(double) * 2 * n_views, stream);
+  dim3 grid((max_width + TW - 1) / TW, (max_height + TH - 1) / TH, n_views);
+  count_launch();
+  k_loss<<<grid, kThreads, sizeof(LossSmem), stream>>>(rendered, target, views, n_views, lp,
+                                                       grad_out, sums);
+  count_launch();
+  k_loss_finalize<<<1, 32, 0, stream>>>(sums, views, n_views, lp.ssim_weight, lp.mode,
+                                        per_view, total);
+}
+
+}  // namespace pxs

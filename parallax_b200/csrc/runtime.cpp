@@ -1,0 +1,241 @@
+// runtime.cpp -- the per-batch rasterisation frame: buffers and stage launches.
+#include "runtime.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pxs {
+
+int g_fail_allocation_after = 0;
+int64_t g_kernel_launches = 0;
+
+void check_cuda(cudaError_t err, const char* what) {
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(PXS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+  }
+}
+
+int bits_for(int64_t count) {
+  int bits = 1;
+  while (bits < 40 && (int64_t(1) << bits) < count) ++bits;
+  return bits;
+}
+
+// ssimKernel (SplatRaster.cpp:587-600), with the same libm expf as the reference.
+void ssim_kernel_weights(float out[11]) {
+  float total = 0.f;
+  for (int i = -5; i <= 5; ++i) {
+    const float v = std::exp(-0.5f * static_cast<float>(i * i) / (1.5f * 1.5f));
+    out[i + 5] = v;
+    total += v;
+  }
+  for (int i = 0; i < 11; ++i) out[i] /= total;
+}
+
+ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_options& options,
+                     int cloud_sh_degree) {
+  ViewBatch b;
+  b.views.resize(static_cast<size_t>(n_views));
+  int tile_offset = 0;
+  int64_t pixel_offset = 0;
+  for (int v = 0; v < n_views; ++v) {
+    ViewDesc& d = b.views[static_cast<size_t>(v)];
+    std::memset(&d, 0, sizeof(d));
+    d.cam = cameras[v];
+    if (d.cam.width < 0 || d.cam.height < 0) throw Error(PXS_ERR_INVALID, "negative image size");
+    for (int c = 0; c < 3; ++c) d.background[c] = options.background[c];
+    d.sh_degree = std::min(options.sh_degree, cloud_sh_degree);
+    d.tiles_x = (d.cam.width + kTile - 1) / kTile;
+    d.tiles_y = (d.cam.height + kTile - 1) / kTile;
+    if (d.tiles_x > 0xFFFF || d.tiles_y > 0xFFFF) throw Error(PXS_ERR_INVALID, "image too large");
+    d.tile_offset = tile_offset;
+    d.pixel_offset = pixel_offset;
+    d.target_offset = pixel_offset;
+    d.min_alpha = options.min_alpha;
+    d.transmittance_cutoff = options.transmittance_cutoff;
+    d.screen_dilation = options.screen_dilation;
+    tile_offset += d.tiles_x * d.tiles_y;
+    pixel_offset += static_cast<int64_t>(d.cam.width) * d.cam.height;
+    b.max_width = std::max(b.max_width, d.cam.width);
+    b.max_height = std::max(b.max_height, d.cam.height);
+  }
+  b.total_pixels = pixel_offset;
+  b.total_tiles = tile_offset;
+  return b;
+}
+
+void Frame::ensure_scan_scratch(int64_t n) {
+  if (n <= scan_capacity_) return;
+  const size_t bytes = scan_scratch_bytes(n) + 64;
+  char* base = scan_scratch.reserve(bytes);
+  scan_ = ScanScratch();
+  scan_scratch_assign(scan_, base, n);
+  scan_capacity_ = n;
+}
+
+void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
+  if (!configured_) {
+    configure_loss_kernel();
+    PXS_CUDA(cudaGetLastError());
+    configured_ = true;
+  }
+  batch = b;
+  N = n;
+  S = s;
+  V = static_cast<int>(b.views.size());
+  slot_stride = round_up(std::max(N, 1), kSortTile);
+  const size_t slots = static_cast<size_t>(V) * static_cast<size_t>(slot_stride);
+  d_views.reserve(static_cast<size_t>(std::max(V, 1)));
+  if (V > 0)
+    PXS_CUDA(cudaMemcpyAsync(d_views.get(), batch.views.data(), sizeof(ViewDesc) * V,
+                             cudaMemcpyHostToDevice, stream));
+  xy.reserve(slots);
+  conic_op.reserve(slots);
+  color.reserve(slots);
+  depth_key.reserve(slots);
+  rect.reserve(slots);
+  tile_count.reserve(slots);
+  sort_keys.reserve(slots);
+  sort_vals.reserve(slots);
+  sort_keys_alt.reserve(slots);
+  sort_vals_alt.reserve(slots);
+  counts.reserve(slots);
+  pair_offsets.reserve(slots);
+  d_total_pairs.reserve(1);
+  screen.reserve(slots);
+  overflow.reserve(1);
+  const size_t pixels = static_cast<size_t>(std::max<int64_t>(batch.total_pixels, 1));
+  rgb.reserve(pixels * 3);
+  dL.reserve(pixels * 3);
+  transmittance.reserve(pixels);
+  last.reserve(pixels);
+  ranges.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  loss_sums.reserve(static_cast<size_t>(2 * std::max(V, 1)));
+  loss_per_view.reserve(static_cast<size_t>(std::max(V, 1)));
+  loss_total.reserve(1);
+  // the depth sort's histograms; the tile sort's are sized in reserve_pairs
+  const size_t depth_hist = radix_hist_entries(static_cast<int64_t>(slots), slot_stride, 8);
+  if (hist.capacity() < depth_hist) {
+    hist.reserve(depth_hist);
+    hist_scanned.reserve(depth_hist);
+  }
+  ensure_scan_scratch(std::max<int64_t>(static_cast<int64_t>(slots),
+                                        static_cast<int64_t>(hist.capacity())));
+}
+
+void Frame::reserve_pairs(int64_t capacity) {
+  if (capacity > INT32_MAX) throw Error(PXS_ERR_CAPACITY, "more than 2^31 tile pairs");
+  if (capacity <= pair_capacity && pair_keys.get() != nullptr) return;
+  const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
+  pair_keys.reserve(cap);
+  pair_vals.reserve(cap);
+  pair_keys_alt.reserve(cap);
+  pair_vals_alt.reserve(cap);
+  pair_capacity = static_cast<int64_t>(cap);
+  const size_t tile_hist = radix_hist_entries(pair_capacity, 0, 9);
+  if (hist.capacity() < tile_hist) {
+    hist.reserve(tile_hist);
+    hist_scanned.reserve(tile_hist);
+  }
+  ensure_scan_scratch(static_cast<int64_t>(hist.capacity()));
+}
+
+void Frame::project(const float* params, cudaStream_t stream, bool want_debug) {
+  ProjectedSoA out;
+  out.xy = xy.get();
+  out.conic_op = conic_op.get();
+  out.color = color.get();
+  out.depth_key = depth_key.get();
+  out.rect = rect.get();
+  out.tile_count = tile_count.get();
+  out.debug_cov = nullptr;
+  if (want_debug) out.debug_cov = debug_cov.reserve(static_cast<size_t>(V) * slot_stride);
+  launch_project(params, N, S, slot_stride, d_views.get(), V, out, stream);
+  PXS_CUDA(cudaGetLastError());
+}
+
+int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
+  const int64_t slots = static_cast<int64_t>(V) * slot_stride;
+  if (slots == 0) {
+    last_pair_count = 0;
+    return 0;
+  }
+  PXS_CUDA(cudaMemcpyAsync(sort_keys.get(), depth_key.get(), sizeof(uint32_t) * slots,
+                           cudaMemcpyDeviceToDevice, stream));
+  launch_iota(sort_vals.get(), slots, stream);
+  uint32_t *k = sort_keys.get(), *v = sort_vals.get();
+  uint32_t *ka = sort_keys_alt.get(), *va = sort_vals_alt.get();
+  radix_sort_pairs(k, v, ka, va, slots, slot_stride, 32, hist.get(), hist_scanned.get(), scan_,
+                   stream);
+  sorted_slots = v;
+  launch_gather_counts(v, tile_count.get(), slots, counts.get(), stream);
+  exclusive_scan_i32_to_i64(counts.get(), pair_offsets.get(), slots, d_total_pairs.get(), scan_,
+                            stream);
+  PXS_CUDA(cudaGetLastError());
+  int64_t K = -1;
+  if (host_sync) {
+    PXS_CUDA(cudaMemcpyAsync(&last_pair_count, d_total_pairs.get(), sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, stream));
+    PXS_CUDA(cudaStreamSynchronize(stream));
+    K = last_pair_count;
+    if (K > pair_capacity) reserve_pairs(K + K / 8 + 1024);
+  } else if (pair_keys.get() == nullptr) {
+    throw Error(PXS_ERR_INVALID, "pair buffers must be reserved before an unsynchronised bin");
+  }
+  PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
+  const uint32_t n_tiles = static_cast<uint32_t>(batch.total_tiles);
+  launch_emit_pairs(v, counts.get(), pair_offsets.get(), rect.get(), d_views.get(), slot_stride,
+                    slots, pair_keys.get(), pair_vals.get(), pair_capacity, n_tiles,
+                    overflow.get(), stream);
+  uint32_t *pk = pair_keys.get(), *pv = pair_vals.get();
+  uint32_t *pka = pair_keys_alt.get(), *pva = pair_vals_alt.get();
+  const int64_t n_sort = host_sync ? K : pair_capacity;
+  const int64_t* n_dev = host_sync ? nullptr : d_total_pairs.get();
+  // one spare key value above the last tile: the overflow sentinel
+  radix_sort_pairs(pk, pv, pka, pva, n_sort, 0, bits_for(int64_t(batch.total_tiles) + 1),
+                   hist.get(), hist_scanned.get(), scan_, stream, n_dev);
+  sorted_pair_keys = pk;
+  sorted_pair_vals = pv;
+  PXS_CUDA(cudaMemsetAsync(ranges.get(), 0, sizeof(int2) * std::max(batch.total_tiles, 1),
+                           stream));
+  launch_tile_ranges(pk, n_sort, n_dev, n_tiles, ranges.get(), stream);
+  PXS_CUDA(cudaGetLastError());
+  return K;
+}
+
+void Frame::forward(cudaStream_t stream, unsigned long long* counts) {
+  launch_forward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
+                 d_views.get(), V, batch.total_tiles, rgb.get(), transmittance.get(), last.get(),
+                 stream, counts);
+  PXS_CUDA(cudaGetLastError());
+}
+
+void Frame::loss(const float* target, float ssim_weight, int mode, float* grad_out,
+                 cudaStream_t stream) {
+  LossParams lp;
+  ssim_kernel_weights(lp.kernel);
+  lp.ssim_weight = ssim_weight;
+  lp.mode = mode;
+  launch_loss(rgb.get(), target, d_views.get(), V, batch.max_width, batch.max_height, lp,
+              grad_out, loss_sums.get(), loss_per_view.get(), loss_total.get(), stream);
+  PXS_CUDA(cudaGetLastError());
+}
+
+void Frame::backward(const float* dL_drgb, cudaStream_t stream) {
+  const size_t slots = static_cast<size_t>(V) * static_cast<size_t>(slot_stride);
+  PXS_CUDA(cudaMemsetAsync(screen.get(), 0, sizeof(ScreenGrad) * slots, stream));
+  launch_backward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
+                  d_views.get(), V, batch.total_tiles, transmittance.get(), last.get(), dL_drgb,
+                  screen.get(), stream);
+  PXS_CUDA(cudaGetLastError());
+}
+
+void Frame::param_grads(const float* params, float* grads, float* screen_gradient,
+                        int32_t* visible_count, cudaStream_t stream) {
+  launch_param_grads(params, N, S, slot_stride, d_views.get(), V, depth_key.get(), conic_op.get(),
+                     color.get(), screen.get(), grads, screen_gradient, visible_count, stream);
+  PXS_CUDA(cudaGetLastError());
+}
+
+}  // namespace pxs

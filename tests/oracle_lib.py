@@ -320,6 +320,14 @@ def orbit_views(count: int, width: int, height: int, radius: float = 3.0, fov: f
 # ------------------------------------------------------------ oracle calls
 
 
+# pxo_splat_f64 with its C alignment padding
+PROJECTED_F64_DTYPE = np.dtype([
+    ("index", np.int32), ("mean", np.float64, 2), ("cov2d", np.float64, 3),
+    ("conic", np.float64, 3), ("depth", np.float64), ("radius", np.float64),
+    ("color", np.float64, 3), ("opacity", np.float64), ("clamped", np.uint32)], align=True)
+assert PROJECTED_F64_DTYPE.itemsize == 128
+
+
 def options(**kw) -> RasterOptions:
     return RasterOptions(**kw)
 

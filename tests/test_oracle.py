@@ -212,11 +212,7 @@ def test_f64_oracle_gradient_matches_central_differences():
     w64 = weights.astype(np.float64)
     lib = O.pxo()
     n = p64.shape[1]
-    proj = np.zeros(n, dtype=[("index", np.int32), ("mean", np.float64, 2),
-                              ("cov2d", np.float64, 3), ("conic", np.float64, 3),
-                              ("depth", np.float64), ("radius", np.float64),
-                              ("color", np.float64, 3), ("opacity", np.float64),
-                              ("clamped", np.uint32)])
+    proj = np.zeros(n, dtype=O.PROJECTED_F64_DTYPE)
     opt_ = opt
     count = lib.pxo_project_f64(as_ptr(p64), n, rest, 2, ct.byref(cam), ct.byref(opt_),
                                 as_ptr(proj))
