@@ -22,6 +22,9 @@ constexpr int kSortTile = kSortThreads * kSortItemsPerThread;
 
 constexpr uint32_t kCulledKey = 0xFFFFFFFFu;
 
+// Widest image, in tiles, the row-binning kernels stage in shared memory.
+constexpr int kMaxTilesX = 2048;
+
 // Everything a kernel needs to know about one view of a batch.
 struct ViewDesc {
   pxs_camera cam;
@@ -29,7 +32,7 @@ struct ViewDesc {
   int32_t sh_degree;         // min(options.sh_degree, cloud sh_degree)
   int32_t tiles_x, tiles_y;
   int32_t tile_offset;       // first global tile id of this view
-  int32_t pad0;
+  int32_t row_offset;        // first global tile-row id of this view
   int64_t pixel_offset;      // first pixel of this view in the image arrays
   float min_alpha;
   float transmittance_cutoff;

@@ -58,14 +58,29 @@ int radix_sort_pairs(uint32_t*& keys, uint32_t*& vals, uint32_t*& keys_alt,
 void launch_iota(uint32_t* out, int64_t n, cudaStream_t stream);
 void launch_gather_counts(const uint32_t* sorted_slots, const int32_t* tile_count, int64_t n,
                           int32_t* counts, cudaStream_t stream);
-void launch_emit_pairs(const uint32_t* sorted_slots, const int32_t* counts,
-                       const int64_t* offsets, const uint2* rect, const ViewDesc* views,
-                       int64_t slot_stride, int64_t n, uint32_t* keys, uint32_t* vals,
-                       int64_t capacity, uint32_t sentinel_tile, int32_t* overflow,
-                       cudaStream_t stream);
 // n is an upper bound when n_device (the device-side pair count) is given.
 void launch_tile_ranges(const uint32_t* keys, int64_t n, const int64_t* n_device,
                         uint32_t n_tiles, int2* ranges, cudaStream_t stream);
+
+// bin.cu
+void configure_bin_kernels();  // once per device, outside graph capture
+void launch_gather_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
+                              const uint2* rect, int64_t n, int32_t* counts,
+                              cudaStream_t stream);
+void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const int64_t* offsets,
+                      const uint2* rect, const ViewDesc* views, int64_t slot_stride, int64_t n,
+                      uint32_t* keys, uint32_t* vals, int64_t capacity, uint32_t sentinel_row,
+                      int32_t* overflow, cudaStream_t stream);
+void launch_row_counts(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+                       const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
+                       int32_t* warp_base, int32_t* tile_counts, cudaStream_t stream);
+void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, int64_t n_tiles,
+                                int64_t capacity, int2* ranges, int32_t* overflow,
+                                cudaStream_t stream);
+void launch_row_expand(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+                       const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
+                       const int32_t* warp_base, const int64_t* tile_offsets, int64_t capacity,
+                       uint32_t* tile_slots, cudaStream_t stream);
 
 // raster.cu
 void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,

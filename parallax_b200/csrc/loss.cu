@@ -8,9 +8,9 @@
 // onto a 5-pixel halo, forms the SSIM map and its three partials there
 // (zero outside the image, as the reference's zero-padded adjoint requires),
 // blurs the five partial planes back onto the tile and writes dL/drgb.
-// Sums run in the reference's tap order and the file is compiled with
-// -fmad=false, so each per-pixel value rounds as the reference's does; the
-// scalar totals are accumulated in double.
+// Each blur pass is register-blocked: a thread loads a strip once and slides
+// the 11 taps along it. Sums run in the reference's tap order (fused
+// multiply-adds allowed); the scalar totals are accumulated in double.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -75,109 +75,153 @@ __global__ void __launch_bounds__(kThreads)
 
   for (int c = 0; c < 3; ++c) {
     if (want_ssim) {
-      // horizontal blur of the five products, every input row, stats columns
-      for (int i = tid; i < IH * SW; i += kThreads) {
-        const int r = i / SW, col = i % SW;
-        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f;
+      // horizontal blur of the five products over every input row, onto the
+      // statistics columns; a thread slides the 11 taps over 6 outputs
+      constexpr int HS = 6;
+      for (int item = tid; item < IH * (SW / HS); item += kThreads) {
+        const int r = item / (SW / HS), col0 = (item % (SW / HS)) * HS;
+        float xs[HS + 10], ys[HS + 10];
 #pragma unroll
-        for (int k = 0; k < 11; ++k) {
-          const float x = sm.in_r[c][r][col + k], y = sm.in_t[c][r][col + k];
-          const float kk = lp.kernel[k];
-          s0 += kk * x;
-          s1 += kk * y;
-          s2 += kk * (x * x);
-          s3 += kk * (y * y);
-          s4 += kk * (x * y);
+        for (int k = 0; k < HS + 10; ++k) {
+          xs[k] = sm.in_r[c][r][col0 + k];
+          ys[k] = sm.in_t[c][r][col0 + k];
         }
-        sm.hb[0][r][col] = s0;
-        sm.hb[1][r][col] = s1;
-        sm.hb[2][r][col] = s2;
-        sm.hb[3][r][col] = s3;
-        sm.hb[4][r][col] = s4;
+#pragma unroll
+        for (int o = 0; o < HS; ++o) {
+          float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) {
+            const float x = xs[o + k], y = ys[o + k], kk = lp.kernel[k];
+            s0 += kk * x;
+            s1 += kk * y;
+            s2 += kk * (x * x);
+            s3 += kk * (y * y);
+            s4 += kk * (x * y);
+          }
+          sm.hb[0][r][col0 + o] = s0;
+          sm.hb[1][r][col0 + o] = s1;
+          sm.hb[2][r][col0 + o] = s2;
+          sm.hb[3][r][col0 + o] = s3;
+          sm.hb[4][r][col0 + o] = s4;
+        }
       }
       __syncthreads();
-      // vertical blur -> statistics, then the SSIM map and its partials in place
-      for (int i = tid; i < SH * SW; i += kThreads) {
-        const int r = i / SW, col = i % SW;
-        float m[5];
+      // vertical blur -> statistics, then the SSIM map and its partials in
+      // place; a thread takes one column and 4 consecutive rows
+      constexpr int VS = 4;
+      constexpr int VSEG = (SH + VS - 1) / VS;
+      for (int item = tid; item < SW * VSEG; item += kThreads) {
+        const int col = item % SW, r0 = (item / SW) * VS;
+        float m[5][VS];
 #pragma unroll
         for (int p = 0; p < 5; ++p) {
-          float s = 0.f;
+          float hv[VS + 10];
 #pragma unroll
-          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.hb[p][r + k][col];
-          m[p] = s;
+          for (int k = 0; k < VS + 10; ++k) hv[k] = (r0 + k < IH) ? sm.hb[p][r0 + k][col] : 0.f;
+#pragma unroll
+          for (int o = 0; o < VS; ++o) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 11; ++k) acc += lp.kernel[k] * hv[o + k];
+            m[p][o] = acc;
+          }
         }
-        const int X = ox - 5 + col, Y = oy - 5 + r;
-        float t_mu = 0.f, t_var = 0.f, t_cov = 0.f, mu_x = m[0], mu_y = m[1];
-        if (X >= 0 && X < W && Y >= 0 && Y < H) {
-          const float var_x = m[2] - mu_x * mu_x;
-          const float var_y = m[3] - mu_y * mu_y;
-          const float cov = m[4] - mu_x * mu_y;
-          const float a = 2.f * mu_x * mu_y + c1;
-          const float b = 2.f * cov + c2;
-          const float cc = mu_x * mu_x + mu_y * mu_y + c1;
-          const float d = var_x + var_y + c2;
-          if (col >= 5 && col < 5 + TW && r >= 5 && r < 5 + TH) ssim_sum += (double)((a * b) / (cc * d));
-          t_mu = scale * (2.f * mu_y * b / (cc * d) - 2.f * mu_x * a * b / (cc * cc * d));
-          t_var = scale * (-(a * b) / (cc * d * d));
-          t_cov = scale * (2.f * a / (cc * d));
-        } else {
-          mu_x = 0.f;
-          mu_y = 0.f;
+#pragma unroll
+        for (int o = 0; o < VS; ++o) {
+          const int r = r0 + o;
+          if (r >= SH) break;
+          const int X = ox - 5 + col, Y = oy - 5 + r;
+          float t_mu = 0.f, t_var = 0.f, t_cov = 0.f, mu_x = m[0][o], mu_y = m[1][o];
+          if (X >= 0 && X < W && Y >= 0 && Y < H) {
+            const float var_x = m[2][o] - mu_x * mu_x;
+            const float var_y = m[3][o] - mu_y * mu_y;
+            const float cov = m[4][o] - mu_x * mu_y;
+            const float a = 2.f * mu_x * mu_y + c1;
+            const float b = 2.f * cov + c2;
+            const float cc = mu_x * mu_x + mu_y * mu_y + c1;
+            const float d = var_x + var_y + c2;
+            if (col >= 5 && col < 5 + TW && r >= 5 && r < 5 + TH)
+              ssim_sum += (double)((a * b) / (cc * d));
+            t_mu = scale * (2.f * mu_y * b / (cc * d) - 2.f * mu_x * a * b / (cc * cc * d));
+            t_var = scale * (-(a * b) / (cc * d * d));
+            t_cov = scale * (2.f * a / (cc * d));
+          } else {
+            mu_x = 0.f;
+            mu_y = 0.f;
+          }
+          sm.st[0][r][col] = t_mu;
+          sm.st[1][r][col] = t_var;
+          sm.st[2][r][col] = t_var * mu_x;
+          sm.st[3][r][col] = t_cov;
+          sm.st[4][r][col] = t_cov * mu_y;
         }
-        sm.st[0][r][col] = t_mu;
-        sm.st[1][r][col] = t_var;
-        sm.st[2][r][col] = t_var * mu_x;
-        sm.st[3][r][col] = t_cov;
-        sm.st[4][r][col] = t_cov * mu_y;
       }
       __syncthreads();
-      // horizontal blur of the partials onto the tile's columns
-      for (int i = tid; i < SH * TW; i += kThreads) {
-        const int r = i / TW, col = i % TW;
+      // horizontal blur of the partials onto the tile's columns, 8 per thread
+      constexpr int HS2 = 8;
+      for (int item = tid; item < 5 * SH * (TW / HS2); item += kThreads) {
+        const int p = item / (SH * (TW / HS2));
+        const int rem = item % (SH * (TW / HS2));
+        const int r = rem / (TW / HS2), col0 = (rem % (TW / HS2)) * HS2;
+        float tv[HS2 + 10];
 #pragma unroll
-        for (int p = 0; p < 5; ++p) {
-          float s = 0.f;
+        for (int k = 0; k < HS2 + 10; ++k) tv[k] = sm.st[p][r][col0 + k];
 #pragma unroll
-          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.st[p][r][col + k];
-          sm.hb[p][r][col] = s;
+        for (int o = 0; o < HS2; ++o) {
+          float acc = 0.f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) acc += lp.kernel[k] * tv[o + k];
+          sm.hb[p][r][col0 + o] = acc;
         }
       }
       __syncthreads();
     }
-    // vertical blur and the gradient at each tile pixel
-    for (int i = tid; i < TH * TW; i += kThreads) {
-      const int r = i / TW, col = i % TW;
-      const int X = ox + col, Y = oy + r;
-      if (X >= W || Y >= H) continue;
-      const float x = sm.in_r[c][r + 10][col + 10];
-      const float y = sm.in_t[c][r + 10][col + 10];
-      float d = 0.f;
+    // vertical blur and the gradient, one column and 2 rows per thread
+    constexpr int VS2 = 2;
+    for (int item = tid; item < TW * (TH / VS2); item += kThreads) {
+      const int col = item % TW, r0 = (item / TW) * VS2;
+      float B[5][VS2];
       if (want_ssim) {
-        float B[5];
 #pragma unroll
         for (int p = 0; p < 5; ++p) {
-          float s = 0.f;
+          float hv[VS2 + 10];
 #pragma unroll
-          for (int k = 0; k < 11; ++k) s += lp.kernel[k] * sm.hb[p][r + k][col];
-          B[p] = s;
+          for (int k = 0; k < VS2 + 10; ++k) hv[k] = sm.hb[p][r0 + k][col];
+#pragma unroll
+          for (int o = 0; o < VS2; ++o) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 11; ++k) acc += lp.kernel[k] * hv[o + k];
+            B[p][o] = acc;
+          }
         }
-        d = 0.f + B[0];
-        d += 2.f * x * B[1];
-        d -= 2.f * B[2];
-        d += y * B[3];
-        d -= B[4];
       }
-      const int64_t o = (pix0 + (int64_t)Y * W + X) * 3 + c;
-      if (lp.mode == 1) {
-        grad_out[o] = d;
-      } else {
-        const float diff = x - y;
-        l1_sum += (double)fabsf(diff);
-        const float sign = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
-        float g = (1.f - w) * sign * inv;
-        if (w > 0.f) g -= w * d;
-        if (grad_out != nullptr) grad_out[o] = g;
+#pragma unroll
+      for (int o = 0; o < VS2; ++o) {
+        const int r = r0 + o;
+        const int X = ox + col, Y = oy + r;
+        if (X >= W || Y >= H) continue;
+        const float x = sm.in_r[c][r + 10][col + 10];
+        const float y = sm.in_t[c][r + 10][col + 10];
+        float d = 0.f;
+        if (want_ssim) {
+          d = B[0][o];
+          d += 2.f * x * B[1][o];
+          d -= 2.f * B[2][o];
+          d += y * B[3][o];
+          d -= B[4][o];
+        }
+        const int64_t oidx = (pix0 + (int64_t)Y * W + X) * 3 + c;
+        if (lp.mode == 1) {
+          grad_out[oidx] = d;
+        } else {
+          const float diff = x - y;
+          l1_sum += (double)fabsf(diff);
+          const float sign = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
+          float g = (1.f - w) * sign * inv;
+          if (w > 0.f) g -= w * d;
+          if (grad_out != nullptr) grad_out[oidx] = g;
+        }
       }
     }
     __syncthreads();

@@ -37,7 +37,7 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
                      int cloud_sh_degree) {
   ViewBatch b;
   b.views.resize(static_cast<size_t>(n_views));
-  int tile_offset = 0;
+  int tile_offset = 0, row_offset = 0;
   int64_t pixel_offset = 0;
   for (int v = 0; v < n_views; ++v) {
     ViewDesc& d = b.views[static_cast<size_t>(v)];
@@ -48,20 +48,25 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
     d.sh_degree = std::min(options.sh_degree, cloud_sh_degree);
     d.tiles_x = (d.cam.width + kTile - 1) / kTile;
     d.tiles_y = (d.cam.height + kTile - 1) / kTile;
-    if (d.tiles_x > 0xFFFF || d.tiles_y > 0xFFFF) throw Error(PXS_ERR_INVALID, "image too large");
+    if (d.tiles_x > kMaxTilesX || d.tiles_y > 0xFFFF)
+      throw Error(PXS_ERR_INVALID, "image too large (at most 2048 tiles across)");
     d.tile_offset = tile_offset;
+    d.row_offset = row_offset;
     d.pixel_offset = pixel_offset;
     d.target_offset = pixel_offset;
     d.min_alpha = options.min_alpha;
     d.transmittance_cutoff = options.transmittance_cutoff;
     d.screen_dilation = options.screen_dilation;
     tile_offset += d.tiles_x * d.tiles_y;
+    row_offset += d.tiles_y;
+    b.max_tiles_x = std::max(b.max_tiles_x, d.tiles_x);
     pixel_offset += static_cast<int64_t>(d.cam.width) * d.cam.height;
     b.max_width = std::max(b.max_width, d.cam.width);
     b.max_height = std::max(b.max_height, d.cam.height);
   }
   b.total_pixels = pixel_offset;
   b.total_tiles = tile_offset;
+  b.total_rows = row_offset;
   return b;
 }
 
@@ -77,6 +82,7 @@ void Frame::ensure_scan_scratch(int64_t n) {
 void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   if (!configured_) {
     configure_loss_kernel();
+    configure_bin_kernels();
     PXS_CUDA(cudaGetLastError());
     configured_ = true;
   }
@@ -111,6 +117,12 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   transmittance.reserve(pixels);
   last.reserve(pixels);
   ranges.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  tile_counts.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  tile_offsets.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  row_ranges.reserve(static_cast<size_t>(std::max(batch.total_rows, 1)));
+  warp_base.reserve(static_cast<size_t>(std::max(batch.total_rows, 1)) * 8 *
+                    static_cast<size_t>(std::max(batch.max_tiles_x, 1)));
+  d_total_records.reserve(1);
   loss_sums.reserve(static_cast<size_t>(2 * std::max(V, 1)));
   loss_per_view.reserve(static_cast<size_t>(std::max(V, 1)));
   loss_total.reserve(1);
@@ -120,23 +132,32 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
     hist.reserve(depth_hist);
     hist_scanned.reserve(depth_hist);
   }
-  ensure_scan_scratch(std::max<int64_t>(static_cast<int64_t>(slots),
-                                        static_cast<int64_t>(hist.capacity())));
+  ensure_scan_scratch(std::max<int64_t>(std::max<int64_t>(static_cast<int64_t>(slots),
+                                                          static_cast<int64_t>(hist.capacity())),
+                                        batch.total_tiles));
 }
 
 void Frame::reserve_pairs(int64_t capacity) {
   if (capacity > INT32_MAX) throw Error(PXS_ERR_CAPACITY, "more than 2^31 tile pairs");
-  if (capacity <= pair_capacity && pair_keys.get() != nullptr) return;
+  if (capacity <= pair_capacity && tile_slots.get() != nullptr) return;
   const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
-  pair_keys.reserve(cap);
-  pair_vals.reserve(cap);
-  pair_keys_alt.reserve(cap);
-  pair_vals_alt.reserve(cap);
+  tile_slots.reserve(cap);
   pair_capacity = static_cast<int64_t>(cap);
-  const size_t tile_hist = radix_hist_entries(pair_capacity, 0, 9);
-  if (hist.capacity() < tile_hist) {
-    hist.reserve(tile_hist);
-    hist_scanned.reserve(tile_hist);
+}
+
+void Frame::reserve_records(int64_t capacity) {
+  if (capacity > INT32_MAX) throw Error(PXS_ERR_CAPACITY, "more than 2^31 tile-row records");
+  if (capacity <= record_capacity && rec_keys.get() != nullptr) return;
+  const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
+  rec_keys.reserve(cap);
+  rec_vals.reserve(cap);
+  rec_keys_alt.reserve(cap);
+  rec_vals_alt.reserve(cap);
+  record_capacity = static_cast<int64_t>(cap);
+  const size_t rec_hist = radix_hist_entries(record_capacity, 0, 9);
+  if (hist.capacity() < rec_hist) {
+    hist.reserve(rec_hist);
+    hist_scanned.reserve(rec_hist);
   }
   ensure_scan_scratch(static_cast<int64_t>(hist.capacity()));
 }
@@ -161,6 +182,7 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
     last_pair_count = 0;
     return 0;
   }
+  // 1. every slot near to far within its view (stable: equal depths by index)
   PXS_CUDA(cudaMemcpyAsync(sort_keys.get(), depth_key.get(), sizeof(uint32_t) * slots,
                            cudaMemcpyDeviceToDevice, stream));
   launch_iota(sort_vals.get(), slots, stream);
@@ -169,9 +191,40 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   radix_sort_pairs(k, v, ka, va, slots, slot_stride, 32, hist.get(), hist_scanned.get(), scan_,
                    stream);
   sorted_slots = v;
-  launch_gather_counts(v, tile_count.get(), slots, counts.get(), stream);
-  exclusive_scan_i32_to_i64(counts.get(), pair_offsets.get(), slots, d_total_pairs.get(), scan_,
-                            stream);
+  // 2. one record per covered tile row, in that order
+  launch_gather_row_counts(v, tile_count.get(), rect.get(), slots, counts.get(), stream);
+  exclusive_scan_i32_to_i64(counts.get(), pair_offsets.get(), slots, d_total_records.get(),
+                            scan_, stream);
+  PXS_CUDA(cudaGetLastError());
+  if (host_sync) {
+    PXS_CUDA(cudaMemcpyAsync(&last_record_count, d_total_records.get(), sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, stream));
+    PXS_CUDA(cudaStreamSynchronize(stream));
+    if (last_record_count > record_capacity)
+      reserve_records(last_record_count + last_record_count / 8 + 1024);
+  } else if (rec_keys.get() == nullptr || tile_slots.get() == nullptr) {
+    throw Error(PXS_ERR_INVALID, "pair buffers must be reserved before an unsynchronised bin");
+  }
+  PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
+  const uint32_t n_rows = static_cast<uint32_t>(batch.total_rows);
+  launch_emit_rows(v, counts.get(), pair_offsets.get(), rect.get(), d_views.get(), slot_stride,
+                   slots, rec_keys.get(), rec_vals.get(), record_capacity, n_rows,
+                   overflow.get(), stream);
+  // 3. records grouped by row, depth order kept (one spare key: the sentinel)
+  uint32_t *rk = rec_keys.get(), *rv = rec_vals.get();
+  uint32_t *rka = rec_keys_alt.get(), *rva = rec_vals_alt.get();
+  const int64_t n_rec = host_sync ? last_record_count : record_capacity;
+  const int64_t* n_dev = host_sync ? nullptr : d_total_records.get();
+  radix_sort_pairs(rk, rv, rka, rva, n_rec, 0, bits_for(int64_t(batch.total_rows) + 1),
+                   hist.get(), hist_scanned.get(), scan_, stream, n_dev);
+  PXS_CUDA(cudaMemsetAsync(row_ranges.get(), 0, sizeof(int2) * std::max(batch.total_rows, 1),
+                           stream));
+  launch_tile_ranges(rk, n_rec, n_dev, n_rows, row_ranges.get(), stream);
+  // 4. tile lengths per row, their offsets, then the lists themselves
+  launch_row_counts(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
+                    batch.max_tiles_x, warp_base.get(), tile_counts.get(), stream);
+  exclusive_scan_i32_to_i64(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
+                            d_total_pairs.get(), scan_, stream);
   PXS_CUDA(cudaGetLastError());
   int64_t K = -1;
   if (host_sync) {
@@ -180,26 +233,13 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
     PXS_CUDA(cudaStreamSynchronize(stream));
     K = last_pair_count;
     if (K > pair_capacity) reserve_pairs(K + K / 8 + 1024);
-  } else if (pair_keys.get() == nullptr) {
-    throw Error(PXS_ERR_INVALID, "pair buffers must be reserved before an unsynchronised bin");
   }
-  PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
-  const uint32_t n_tiles = static_cast<uint32_t>(batch.total_tiles);
-  launch_emit_pairs(v, counts.get(), pair_offsets.get(), rect.get(), d_views.get(), slot_stride,
-                    slots, pair_keys.get(), pair_vals.get(), pair_capacity, n_tiles,
-                    overflow.get(), stream);
-  uint32_t *pk = pair_keys.get(), *pv = pair_vals.get();
-  uint32_t *pka = pair_keys_alt.get(), *pva = pair_vals_alt.get();
-  const int64_t n_sort = host_sync ? K : pair_capacity;
-  const int64_t* n_dev = host_sync ? nullptr : d_total_pairs.get();
-  // one spare key value above the last tile: the overflow sentinel
-  radix_sort_pairs(pk, pv, pka, pva, n_sort, 0, bits_for(int64_t(batch.total_tiles) + 1),
-                   hist.get(), hist_scanned.get(), scan_, stream, n_dev);
-  sorted_pair_keys = pk;
-  sorted_pair_vals = pv;
-  PXS_CUDA(cudaMemsetAsync(ranges.get(), 0, sizeof(int2) * std::max(batch.total_tiles, 1),
-                           stream));
-  launch_tile_ranges(pk, n_sort, n_dev, n_tiles, ranges.get(), stream);
+  launch_ranges_from_offsets(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
+                             pair_capacity, ranges.get(), overflow.get(), stream);
+  launch_row_expand(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
+                    batch.max_tiles_x, warp_base.get(), tile_offsets.get(), pair_capacity,
+                    tile_slots.get(), stream);
+  sorted_pair_vals = tile_slots.get();
   PXS_CUDA(cudaGetLastError());
   return K;
 }

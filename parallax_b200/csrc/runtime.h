@@ -87,6 +87,8 @@ struct ViewBatch {
   std::vector<ViewDesc> views;
   int64_t total_pixels = 0;
   int total_tiles = 0;
+  int total_rows = 0;       // tile rows over all views
+  int max_tiles_x = 0;
   int max_width = 0, max_height = 0;
 };
 
@@ -116,13 +118,16 @@ class Frame {
   void param_grads(const float* params, float* grads, float* screen_gradient,
                    int32_t* visible_count, cudaStream_t stream);
   void reserve_pairs(int64_t capacity);
+  void reserve_records(int64_t capacity);
 
   // sizes
   int N = 0, S = 0, V = 0;
   int64_t slot_stride = 0;
   ViewBatch batch;
   int64_t pair_capacity = 0;
+  int64_t record_capacity = 0;
   int64_t last_pair_count = 0;
+  int64_t last_record_count = 0;
 
   // device buffers
   DeviceArray<ViewDesc> d_views;
@@ -133,8 +138,12 @@ class Frame {
   DeviceArray<int32_t> tile_count;
   DeviceArray<uint32_t> sort_keys, sort_vals, sort_keys_alt, sort_vals_alt;
   DeviceArray<int32_t> counts;
-  DeviceArray<int64_t> pair_offsets, d_total_pairs;
-  DeviceArray<uint32_t> pair_keys, pair_vals, pair_keys_alt, pair_vals_alt;
+  DeviceArray<int64_t> pair_offsets, d_total_pairs, d_total_records;
+  DeviceArray<uint32_t> rec_keys, rec_vals, rec_keys_alt, rec_vals_alt;  // tile-row records
+  DeviceArray<int2> row_ranges;
+  DeviceArray<int32_t> warp_base, tile_counts;
+  DeviceArray<int64_t> tile_offsets;
+  DeviceArray<uint32_t> tile_slots;  // per-tile key lists (pair_capacity)
   DeviceArray<uint32_t> hist, hist_scanned;
   DeviceArray<char> scan_scratch;
   DeviceArray<int2> ranges;
@@ -145,8 +154,7 @@ class Frame {
   DeviceArray<ScreenGrad> screen;
   DeviceArray<int32_t> overflow;
 
-  // after bin(): where the sorted pairs ended up
-  uint32_t* sorted_pair_keys = nullptr;
+  // after bin(): the per-tile lists and the depth-sorted slots
   uint32_t* sorted_pair_vals = nullptr;
   uint32_t* sorted_slots = nullptr;
 

@@ -1,14 +1,9 @@
-// sort.cu -- tile binning: depth sort, pair emission, tile sort and ranges.
+// sort.cu -- scans, radix sort and key ranges for the binning path.
 //
-// The reference bins splats with a counting sort over tiles of its
-// depth-sorted projected list (SplatRaster.cpp:104-151, :260-261): each tile's
-// list is near to far. Here that order is produced in two stable steps:
-//   1. a stable LSD radix sort of every (view, gaussian) slot by the float bits
-//      of its depth (segmented per view; ties keep gaussian order),
-//   2. pair emission in that order, then a stable LSD radix sort of the pairs
-//      by global tile id (ceil(log2 tiles) bits, two passes of <= 9 bits).
-// The result per tile equals the reference's key list, with equal depths
-// ordered by gaussian index.
+// Device-wide exclusive scans, a stable segmented LSD radix sort of 32-bit
+// keys with 32-bit values, and the range kernel. The binning path uses them
+// for the depth sort of every (view, gaussian) slot (segmented per view; ties
+// keep gaussian order) and for grouping the tile-row records by row (bin.cu).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -118,9 +113,16 @@ __global__ void __launch_bounds__(kSortThreads)
   const int64_t seg_end = min(seg_begin + p.segment_len, n);
   const int64_t begin = seg_begin + (int64_t)bis * kSortTile;
   const uint32_t mask = (uint32_t)bins - 1u;
+  uint32_t key[kSortItemsPerThread];
+#pragma unroll
   for (int k = 0; k < kSortItemsPerThread; ++k) {
     const int64_t i = begin + (int64_t)k * kSortThreads + threadIdx.x;
-    if (i < seg_end && i < begin + kSortTile) atomicAdd(&h[(keys[i] >> p.shift) & mask], 1u);
+    key[k] = i < seg_end ? keys[i] : 0xFFFFFFFFu;
+  }
+#pragma unroll
+  for (int k = 0; k < kSortItemsPerThread; ++k) {
+    const int64_t i = begin + (int64_t)k * kSortThreads + threadIdx.x;
+    if (i < seg_end) atomicAdd(&h[(key[k] >> p.shift) & mask], 1u);
   }
   __syncthreads();
   for (int d = threadIdx.x; d < bins; d += blockDim.x)
@@ -128,14 +130,21 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 // Stable scatter of one block tile. Items are warp-striped (warp w owns
-// [w*512, (w+1)*512), item k of a lane at k*32 + lane), ranked with
-// __match_any_sync per digit, then offset by earlier warps and earlier blocks.
+// [w*512, (w+1)*512), item k of a lane at k*32 + lane) and ranked with
+// __match_any_sync per digit, then offset by earlier warps. The tile is
+// reordered by digit in shared memory and written out digit run by digit run,
+// so consecutive threads write consecutive addresses.
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                       uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                       RadixPass p, const uint32_t* __restrict__ offsets) {
-  __shared__ uint32_t counts[kSortWarps][kMaxBins];
+  // per-warp digit counters; reused as the staging buffer once ranks are known
+  __shared__ uint32_t counts[kSortWarps * kMaxBins];
   __shared__ uint32_t block_offset[kMaxBins];
+  __shared__ uint32_t digit_start[kMaxBins];
+  __shared__ uint32_t warp_sums[32];
+  static_assert(kSortWarps * kMaxBins >= kSortTile, "staging buffer too small");
+  static_assert(2 * kSortThreads >= kMaxBins, "two digits per thread");
   const int bins = 1 << p.bits;
   const uint32_t mask = (uint32_t)bins - 1u;
   const int seg = blockIdx.x / p.blocks_per_segment;
@@ -145,9 +154,10 @@ __global__ void __launch_bounds__(kSortThreads)
   const int64_t seg_end = min(seg_begin + p.segment_len, n);
   const int64_t begin = seg_begin + (int64_t)bis * kSortTile;
   const int64_t end = min(begin + kSortTile, seg_end);
+  const int items = end > begin ? (int)(end - begin) : 0;
   for (int d = threadIdx.x; d < bins; d += blockDim.x) {
 #pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) counts[w][d] = 0;
+    for (int w = 0; w < kSortWarps; ++w) counts[w * kMaxBins + d] = 0;
     block_offset[d] = offsets[((int64_t)seg * bins + d) * p.blocks_per_segment + bis];
   }
   __syncthreads();
@@ -157,10 +167,10 @@ __global__ void __launch_bounds__(kSortThreads)
   int digit[kSortItemsPerThread];
 #pragma unroll
   for (int k = 0; k < kSortItemsPerThread; ++k) {
-    const int64_t i = begin + (int64_t)warp * (kSortItemsPerThread * 32) + k * 32 + lane;
-    const bool valid = i < end;
-    key[k] = valid ? keys_in[i] : 0u;
-    val[k] = valid ? vals_in[i] : 0u;
+    const int local = warp * (kSortItemsPerThread * 32) + k * 32 + lane;
+    const bool valid = local < items;
+    key[k] = valid ? keys_in[begin + local] : 0u;
+    val[k] = valid ? vals_in[begin + local] : 0u;
     digit[k] = valid ? (int)((key[k] >> p.shift) & mask) : kMaxBins;  // sentinel groups invalid
   }
 #pragma unroll
@@ -169,30 +179,69 @@ __global__ void __launch_bounds__(kSortThreads)
     const unsigned peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
-    if (d < kMaxBins) base = counts[warp][d];
+    if (d < kMaxBins) base = counts[warp * kMaxBins + d];
     __syncwarp();
-    if (lane == leader && d < kMaxBins) counts[warp][d] = base + __popc(peers);
+    if (lane == leader && d < kMaxBins) counts[warp * kMaxBins + d] = base + __popc(peers);
     __syncwarp();
     rank[k] = base + __popc(peers & lt);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < bins; d += blockDim.x) {
-    uint32_t run = 0;
+  // thread t owns digits 2t and 2t+1: exclusive prefix over warps in place,
+  // then the block-local start of each digit by a scan in digit order
+  uint32_t total_pair[2] = {0u, 0u};
 #pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t c = counts[w][d];
-      counts[w][d] = run;
-      run += c;
+  for (int r = 0; r < 2; ++r) {
+    const int d = 2 * (int)threadIdx.x + r;
+    if (d < bins) {
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = counts[w * kMaxBins + d];
+        counts[w * kMaxBins + d] = run;
+        run += c;
+      }
+      total_pair[r] = run;
     }
   }
+  uint32_t block_total;
+  const uint32_t start = block_exclusive_scan<uint32_t>(total_pair[0] + total_pair[1],
+                                                         &block_total, warp_sums);
+  if (2 * (int)threadIdx.x < bins) digit_start[2 * threadIdx.x] = start;
+  if (2 * (int)threadIdx.x + 1 < bins) digit_start[2 * threadIdx.x + 1] = start + total_pair[0];
   __syncthreads();
+  uint32_t local_pos[kSortItemsPerThread];
 #pragma unroll
   for (int k = 0; k < kSortItemsPerThread; ++k) {
     const int d = digit[k];
-    if (d >= kMaxBins) continue;
-    const uint32_t pos = block_offset[d] + counts[warp][d] + rank[k];
-    keys_out[pos] = key[k];
-    vals_out[pos] = val[k];
+    local_pos[k] = d < kMaxBins ? digit_start[d] + counts[warp * kMaxBins + d] + rank[k] : 0u;
+  }
+  __syncthreads();  // counts is now free: stage the keys by digit
+  uint32_t* stage = counts;
+#pragma unroll
+  for (int k = 0; k < kSortItemsPerThread; ++k)
+    if (digit[k] < kMaxBins) stage[local_pos[k]] = key[k];
+  __syncthreads();
+  uint32_t global_pos[kSortItemsPerThread];
+#pragma unroll
+  for (int k = 0; k < kSortItemsPerThread; ++k) {
+    const int i = k * kSortThreads + threadIdx.x;
+    global_pos[k] = 0xFFFFFFFFu;
+    if (i < items) {
+      const uint32_t kk = stage[i];
+      const int d = (int)((kk >> p.shift) & mask);
+      global_pos[k] = block_offset[d] + ((uint32_t)i - digit_start[d]);
+      keys_out[global_pos[k]] = kk;
+    }
+  }
+  __syncthreads();  // stage the values the same way
+#pragma unroll
+  for (int k = 0; k < kSortItemsPerThread; ++k)
+    if (digit[k] < kMaxBins) stage[local_pos[k]] = val[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kSortItemsPerThread; ++k) {
+    const int i = k * kSortThreads + threadIdx.x;
+    if (i < items) vals_out[global_pos[k]] = stage[i];
   }
 }
 
@@ -209,55 +258,35 @@ __global__ void k_gather_counts(const uint32_t* __restrict__ sorted_slots,
   if (i < n) counts[i] = tile_count[sorted_slots[i]];
 }
 
-// Writes (global tile id, slot) for every tile of every visible slot, in
-// depth order, each slot's tiles row by row (buildTiles, SplatRaster.cpp:140-149).
-__global__ void k_emit_pairs(const uint32_t* __restrict__ sorted_slots,
-                             const int32_t* __restrict__ counts,
-                             const int64_t* __restrict__ offsets, const uint2* __restrict__ rect,
-                             const ViewDesc* __restrict__ views, int64_t slot_stride, int64_t n,
-                             uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                             int64_t capacity, uint32_t sentinel_tile,
-                             int32_t* __restrict__ overflow) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int cnt = counts[i];
-  if (cnt == 0) return;
-  const int64_t off = offsets[i];
-  if (off + cnt > capacity) {
-    // does not fit: flag it, and fill the part below capacity with sentinel
-    // pairs (tile id = n_tiles, past every real tile) so nothing reads garbage
-    atomicExch(overflow, 1);
-    for (int64_t j = off; j < capacity && j < off + cnt; ++j) {
-      keys[j] = sentinel_tile;
-      vals[j] = 0u;
-    }
-    return;
-  }
-  const uint32_t slot = sorted_slots[i];
-  const int v = (int)(slot / slot_stride);
-  const ViewDesc& vd = views[v];
-  const uint2 r = rect[slot];
-  const int x0 = r.x & 0xFFFF, x1 = r.x >> 16, y0 = r.y & 0xFFFF, y1 = r.y >> 16;
-  int64_t j = off;
-  for (int ty = y0; ty <= y1; ++ty) {
-    const uint32_t row = (uint32_t)(vd.tile_offset + ty * vd.tiles_x);
-    for (int tx = x0; tx <= x1; ++tx, ++j) {
-      keys[j] = row + (uint32_t)tx;
-      vals[j] = slot;
-    }
-  }
-}
-
-__global__ void k_tile_ranges(const uint32_t* __restrict__ keys, int64_t n_max,
-                              const int64_t* __restrict__ n_device, uint32_t n_tiles,
-                              int2* __restrict__ ranges) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256)
+    k_tile_ranges(const uint32_t* __restrict__ keys, int64_t n_max,
+                  const int64_t* __restrict__ n_device, uint32_t n_tiles,
+                  int2* __restrict__ ranges) {
   const int64_t n = n_device != nullptr ? min(*n_device, n_max) : n_max;
-  if (i >= n) return;
-  const uint32_t k = keys[i];
-  if (k >= n_tiles) return;  // overflow sentinels
-  if (i == 0 || keys[i - 1] != k) ranges[k].x = (int)i;
-  if (i == n - 1 || keys[i + 1] != k) ranges[k].y = (int)(i + 1);
+  const int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  uint32_t k[6];  // keys[i0-1 .. i0+4]
+  k[0] = i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu;
+  if (i0 + 4 <= n) {
+    const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
+    k[1] = q.x;
+    k[2] = q.y;
+    k[3] = q.z;
+    k[4] = q.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) k[1 + j] = i0 + j < n ? keys[i0 + j] : 0xFFFFFFFFu;
+  }
+  k[5] = i0 + 4 < n ? keys[i0 + 4] : 0xFFFFFFFFu;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t i = i0 + j;
+    if (i >= n) break;
+    const uint32_t key = k[1 + j];
+    if (key >= n_tiles) continue;  // overflow sentinels
+    if (i == 0 || k[j] != key) ranges[key].x = (int)i;
+    if (i == n - 1 || k[2 + j] != key) ranges[key].y = (int)(i + 1);
+  }
 }
 
 }  // namespace
@@ -374,25 +403,12 @@ void launch_gather_counts(const uint32_t* sorted_slots, const int32_t* tile_coun
   }
 }
 
-void launch_emit_pairs(const uint32_t* sorted_slots, const int32_t* counts,
-                       const int64_t* offsets, const uint2* rect, const ViewDesc* views,
-                       int64_t slot_stride, int64_t n, uint32_t* keys, uint32_t* vals,
-                       int64_t capacity, uint32_t sentinel_tile, int32_t* overflow,
-                       cudaStream_t stream) {
-  if (n > 0) {
-    count_launch();
-    k_emit_pairs<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
-        sorted_slots, counts, offsets, rect, views, slot_stride, n, keys, vals, capacity,
-        sentinel_tile, overflow);
-  }
-}
-
 void launch_tile_ranges(const uint32_t* keys, int64_t n, const int64_t* n_device,
                         uint32_t n_tiles, int2* ranges, cudaStream_t stream) {
   if (n > 0) {
     count_launch();
-    k_tile_ranges<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(keys, n, n_device, n_tiles,
-                                                                   ranges);
+    k_tile_ranges<<<(unsigned)((n + 1023) / 1024), 256, 0, stream>>>(keys, n, n_device, n_tiles,
+                                                                     ranges);
   }
 }
 

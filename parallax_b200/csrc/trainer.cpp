@@ -29,7 +29,7 @@ struct GraphState {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int N = -1, V = -1;
-  int64_t pixels = -1, pair_capacity = -1;
+  int64_t pixels = -1, pair_capacity = -1, record_capacity = -1;
   int tiles = -1;
   int generation = -1;
   bool timing = false;
@@ -40,7 +40,7 @@ struct GraphState {
     exec = nullptr;
     graph = nullptr;
     N = V = tiles = generation = -1;
-    pixels = pair_capacity = -1;
+    pixels = pair_capacity = record_capacity = -1;
   }
 };
 
@@ -383,11 +383,12 @@ struct pxs_trainer {
     const pxs::ViewBatch b = batch_for(views);
     frame.prepare(b, N, S, stream);  // also uploads the view descriptors
     dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
-    if (frame.pair_capacity == 0) {
+    if (frame.pair_capacity == 0 || frame.record_capacity == 0) {
       // learn the pair count once, then run unsynchronised with headroom
       frame.project(params.get(), stream);
       const int64_t K = frame.bin(true, stream);
       frame.reserve_pairs(K + K / 2 + 65536);
+      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
     }
     for (int attempt = 0; attempt < 3; ++attempt) {
       upload_scalars();
@@ -396,6 +397,7 @@ struct pxs_trainer {
                            graph.timing != timing ||
                            graph.pixels != b.total_pixels || graph.tiles != b.total_tiles ||
                            graph.pair_capacity != frame.pair_capacity ||
+                           graph.record_capacity != frame.record_capacity ||
                            graph.generation != generation;
         if (stale) {
           graph.reset();
@@ -416,6 +418,7 @@ struct pxs_trainer {
           graph.pixels = b.total_pixels;
           graph.tiles = b.total_tiles;
           graph.pair_capacity = frame.pair_capacity;
+          graph.record_capacity = frame.record_capacity;
           graph.generation = generation;
           graph.timing = timing;
           graph.launches = pxs::g_kernel_launches - before;
@@ -441,6 +444,7 @@ struct pxs_trainer {
       frame.project(params.get(), stream);
       const int64_t K = frame.bin(true, stream);
       frame.reserve_pairs(K + K / 2 + 65536);
+      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
       graph.reset();
     }
     if (*host_overflow != 0) throw Error(PXS_ERR_CAPACITY, "tile pairs overflowed three times");

@@ -2,10 +2,11 @@
 the reference.
 
 Tolerances, stated per quantity:
-  * projection: depth, mean and the visible set bit-exact; exp-derived values
-    (cov2d, conic, radius, opacity, colour) within 4 ulp -- the oracle uses
-    glibc's expf, the device a correctly rounded exp, and those differ in the
-    last bit for ~0.06% of inputs;
+  * projection: the visible set, its order, depth, mean and clamp flags
+    bit-exact; every other field bit-exact for gaussians whose exp() inputs
+    glibc's expf rounds correctly (the device computes a correctly rounded
+    exp; glibc differs in the last bit for ~0.06% of inputs), and within 1e-5
+    relative (to the matrix scale for cov2d/conic) for the rest;
   * per-tile key lists: identical (equal depths ordered by gaussian index);
   * rendered images: within 1e-5 relative (floor 1e-3) for all but a 1e-3
     fraction of values, whose differences come from a splat crossing the
@@ -13,8 +14,9 @@ Tolerances, stated per quantity:
   * loss: 1e-5 relative; dL/drgb: 1e-5 of its largest magnitude;
   * gradients: 1e-4 relative, normwise per parameter group (the device sums in
     a different order, with atomics);
-  * Adam: bit-exact; densify: counts, sources and the RNG state exact,
-    parameters within 1 ulp.
+  * Adam: bit-exact; densify: counts, sources, the RNG state and all
+    non-position values exact, split-child positions within 1e-6 (glibc's
+    logf/cosf in the normal draw are not always correctly rounded).
 """
 from __future__ import annotations
 
@@ -246,7 +248,9 @@ def test_backward_accumulates_rather_than_overwriting(ctx):
                               once.visible_count.copy())
     px.rasterize_splats_backward(cloud, cam, opt, dL, twice, ctx)
     assert np.array_equal(twice.visible_count, 2 * once.visible_count)
-    assert np.allclose(twice.params, 2 * once.params, rtol=1e-4, atol=1e-12)
+    # the device sums with atomics in no fixed order: compare normwise per group
+    errs = grad_errors(twice.params, 2 * once.params)
+    assert max(errs.values()) <= 1e-5, errs
 
 
 @pytest.mark.parametrize("name", ["raster_sh0.npz", "raster_sh3.npz"])
