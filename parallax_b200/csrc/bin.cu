@@ -8,13 +8,14 @@
 //   1. each visible splat (in depth order) emits one record per tile row it
 //      covers -- (global row id, slot), about one seventh as many as pairs;
 //   2. one stable radix pass groups the records by row, keeping depth order;
-//   3. one CTA per row counts, per column, the records covering it (per warp,
-//      over contiguous eighths of the row's records), which gives every tile's
-//      length; an exclusive scan over the tiles gives the tile ranges;
-//   4. the same CTA walks its records again, 32 at a time per warp: each lane
-//      sets its bit in a per-column bitmap for every column its splat covers,
-//      and the pair's place in the tile's list is the column's running base
-//      plus the number of earlier lanes in the bitmap.
+//   3. each row is cut into chunks of 2048 records; one CTA per chunk counts,
+//      per column, the records covering it; a per-row pass turns those into
+//      each chunk's base within every tile of the row and the tiles' lengths;
+//      an exclusive scan over the tiles gives the tile ranges;
+//   4. one CTA per chunk walks its records again, 32 at a time per warp: each
+//      lane sets its bit in a per-column bitmap for every column its splat
+//      covers, and the pair's place in the tile's list is the column's running
+//      base plus the number of earlier lanes in the bitmap.
 // The result -- ranges and slot lists -- is exactly the reference's, with
 // equal depths in gaussian order (the depth sort is stable over slots).
 #include "common.cuh"
@@ -102,40 +103,136 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Per row: how many of its records cover each column, per warp eighth
-// (warp_base, exclusive over warps) and in total (the tile's length).
+// Rows are cut into chunks of at most kChunk records so the work balances
+// whatever the rows' lengths. chunks[c] = (row, begin, end); n_chunks[0] is
+// the count. One CTA builds the table with a block-wide scan over the rows.
+constexpr int kChunk = 2048;
+constexpr int kPerLane = kChunk / (kWarps * 32);  // records per lane per chunk
+
+__global__ void __launch_bounds__(1024)
+    k_row_chunks(const int2* __restrict__ row_ranges, int total_rows, int max_chunks,
+                 int4* __restrict__ chunks, int32_t* __restrict__ n_chunks) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < total_rows; base += blockDim.x) {
+    const int row = base + threadIdx.x;
+    int len = 0;
+    int2 range = make_int2(0, 0);
+    if (row < total_rows) {
+      range = row_ranges[row];
+      len = max(0, range.y - range.x);
+    }
+    const int count = (len + kChunk - 1) / kChunk;
+    // block-wide inclusive scan of count
+    int x = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int n = __shfl_up_sync(kFull, x, o);
+      if (lane_id() >= o) x += n;
+    }
+    if (lane_id() == 31) warp_sums[warp_id()] = x;
+    __syncthreads();
+    if (warp_id() == 0) {
+      int y = lane_id() < (int)(blockDim.x / 32) ? warp_sums[lane_id()] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(kFull, y, o);
+        if (lane_id() >= o) y += n;
+      }
+      warp_sums[lane_id()] = y;
+    }
+    __syncthreads();
+    const int first = carry + (warp_id() > 0 ? warp_sums[warp_id() - 1] : 0) + x - count;
+    for (int j = 0; j < count; ++j) {
+      const int c = first + j;
+      if (c < max_chunks)
+        chunks[c] = make_int4(row, range.x + j * kChunk, min(range.y, range.x + (j + 1) * kChunk), 0);
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = first + count;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) n_chunks[0] = min(carry, max_chunks);
+}
+
+// Per-warp column counts of one chunk into s_cnt [kWarps][tiles_x] (zeroed by
+// the caller); lanes prefetch their records' rects first.
+__device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32_t* __restrict__ rec_slots,
+                                                    const uint2* __restrict__ rect, int max_tiles_x,
+                                                    int32_t* s_cnt, uint32_t (&slot)[kPerLane],
+                                                    uint32_t (&xr)[kPerLane]) {
+  const int w = warp_id(), lane = lane_id();
+  const int w_begin = ch.y + w * (kChunk / kWarps);
+#pragma unroll
+  for (int k = 0; k < kPerLane; ++k) {
+    const int rec = w_begin + k * 32 + lane;
+    slot[k] = 0u;
+    xr[k] = 1u;  // x0 = 1 > x1 = 0: covers nothing
+    if (rec < ch.z) {
+      slot[k] = rec_slots[rec];
+      xr[k] = rect[slot[k]].x;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kPerLane; ++k) {
+    const int x0 = xr[k] & 0xFFFF, x1 = xr[k] >> 16;
+    for (int c = x0; c <= x1; ++c) atomicAdd(&s_cnt[w * max_tiles_x + c], 1);
+  }
+}
+
+// Per chunk: how many of its records cover each column.
 __global__ void __launch_bounds__(kWarps * 32)
-    k_row_counts(const int2* __restrict__ row_ranges, const uint32_t* __restrict__ rec_slots,
-                 const uint2* __restrict__ rect, const ViewDesc* __restrict__ views, int n_views,
-                 int max_tiles_x, int32_t* __restrict__ warp_base,
-                 int32_t* __restrict__ tile_counts) {
+    k_chunk_counts(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
+                   const uint32_t* __restrict__ rec_slots, const uint2* __restrict__ rect,
+                   const ViewDesc* __restrict__ views, int n_views, int max_tiles_x,
+                   int32_t* __restrict__ chunk_counts) {
   extern __shared__ int32_t s_cnt[];  // [kWarps][max_tiles_x]
+  if ((int)blockIdx.x >= n_chunks[0]) return;
+  const int4 ch = chunks[blockIdx.x];
+  const ViewDesc& vd = views[view_of_row(views, n_views, ch.x)];
+  const int tiles_x = vd.tiles_x;
+  for (int i = threadIdx.x; i < kWarps * tiles_x; i += blockDim.x)
+    s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
+  __syncthreads();
+  uint32_t slot[kPerLane], xr[kPerLane];
+  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, s_cnt, slot, xr);
+  __syncthreads();
+  for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) total += s_cnt[k * max_tiles_x + c];
+    chunk_counts[(int64_t)blockIdx.x * max_tiles_x + c] = total;
+  }
+}
+
+// Per row: each chunk's base within each tile of the row (exclusive over the
+// row's chunks, in order) and the tile's length. The row's chunks are
+// consecutive in the table, found from the first one by a binary search.
+__global__ void __launch_bounds__(256)
+    k_row_tiles(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
+                const ViewDesc* __restrict__ views, int n_views, int max_tiles_x,
+                const int32_t* __restrict__ chunk_counts, int32_t* __restrict__ chunk_base,
+                int32_t* __restrict__ tile_counts) {
   const int row = blockIdx.x;
   const int v = view_of_row(views, n_views, row);
   const ViewDesc& vd = views[v];
   const int tiles_x = vd.tiles_x;
-  const int local_row = row - vd.row_offset;
-  const int2 range = row_ranges[row];
-  for (int i = threadIdx.x; i < kWarps * tiles_x; i += blockDim.x)
-    s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
-  __syncthreads();
-  const int w = warp_id(), lane = lane_id();
-  const int len = max(0, range.y - range.x);
-  const int per = (len + kWarps - 1) / kWarps;
-  const int w_begin = range.x + w * per, w_end = min(range.y, w_begin + per);
-  for (int rec = w_begin + lane; rec < w_end; rec += 32) {
-    const uint2 r = rect[rec_slots[rec]];
-    const int x0 = r.x & 0xFFFF, x1 = r.x >> 16;
-    for (int c = x0; c <= x1; ++c) atomicAdd(&s_cnt[w * max_tiles_x + c], 1);
+  const int nc = n_chunks[0];
+  // first chunk with chunks[c].x >= row
+  int lo = 0, hi = nc;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (chunks[mid].x < row) lo = mid + 1;
+    else hi = mid;
   }
-  __syncthreads();
-  const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)local_row * tiles_x;
+  const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)(row - vd.row_offset) * tiles_x;
   for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
     int run = 0;
-#pragma unroll
-    for (int k = 0; k < kWarps; ++k) {
-      const int t = s_cnt[k * max_tiles_x + c];
-      warp_base[((int64_t)row * kWarps + k) * max_tiles_x + c] = run;
+    for (int k = lo; k < nc && chunks[k].x == row; ++k) {
+      const int t = chunk_counts[(int64_t)k * max_tiles_x + c];
+      chunk_base[(int64_t)k * max_tiles_x + c] = run;
       run += t;
     }
     tile_counts[tile0 + c] = run;
@@ -159,55 +256,59 @@ __global__ void k_ranges_from_offsets(const int32_t* __restrict__ counts,
   }
 }
 
-// Writes each row's records into its tiles' lists, in record (depth) order.
+// Writes each chunk's records into its row's tile lists, in record (depth)
+// order: 32 records at a time per warp, a per-column bitmap giving each pair
+// its place among the lanes.
 __global__ void __launch_bounds__(kWarps * 32)
-    k_row_expand(const int2* __restrict__ row_ranges, const uint32_t* __restrict__ rec_slots,
-                 const uint2* __restrict__ rect, const ViewDesc* __restrict__ views, int n_views,
-                 int max_tiles_x, const int32_t* __restrict__ warp_base,
-                 const int64_t* __restrict__ tile_offsets, int64_t capacity,
-                 uint32_t* __restrict__ tile_slots) {
-  extern __shared__ int32_t s_mem[];  // base [kWarps][max_tiles_x], then bitmap, same shape
-  const int row = blockIdx.x;
-  const int v = view_of_row(views, n_views, row);
-  const ViewDesc& vd = views[v];
+    k_chunk_expand(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
+                   const uint32_t* __restrict__ rec_slots, const uint2* __restrict__ rect,
+                   const ViewDesc* __restrict__ views, int n_views, int max_tiles_x,
+                   const int32_t* __restrict__ chunk_base,
+                   const int64_t* __restrict__ tile_offsets, int64_t capacity,
+                   uint32_t* __restrict__ tile_slots) {
+  extern __shared__ int32_t s_mem[];  // counts/base [kWarps][max_tiles_x], bitmap same shape
+  if ((int)blockIdx.x >= n_chunks[0]) return;
+  const int4 ch = chunks[blockIdx.x];
+  const ViewDesc& vd = views[view_of_row(views, n_views, ch.x)];
   const int tiles_x = vd.tiles_x;
-  const int local_row = row - vd.row_offset;
-  const int2 range = row_ranges[row];
   const int w = warp_id(), lane = lane_id();
-  int32_t* base = s_mem + w * max_tiles_x;
-  uint32_t* bitmap = reinterpret_cast<uint32_t*>(s_mem + kWarps * max_tiles_x) + w * max_tiles_x;
-  const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)local_row * tiles_x;
-  for (int c = lane; c < tiles_x; c += 32) {
-    base[c] = (int32_t)tile_offsets[tile0 + c] +
-              warp_base[((int64_t)row * kWarps + w) * max_tiles_x + c];
-    bitmap[c] = 0u;
+  int32_t* s_cnt = s_mem;
+  uint32_t* bitmap_all = reinterpret_cast<uint32_t*>(s_mem + kWarps * max_tiles_x);
+  for (int i = threadIdx.x; i < kWarps * tiles_x; i += blockDim.x) {
+    s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
+    bitmap_all[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0u;
   }
-  __syncwarp();
-  const int len = max(0, range.y - range.x);
-  const int per = (len + kWarps - 1) / kWarps;
-  const int w_begin = range.x + w * per, w_end = min(range.y, w_begin + per);
+  __syncthreads();
+  uint32_t slot[kPerLane], xr[kPerLane];
+  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, s_cnt, slot, xr);
+  __syncthreads();
+  // per column: exclusive prefix over warps, plus the chunk's base and the tile's offset
+  const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)(ch.x - vd.row_offset) * tiles_x;
+  for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
+    int run = (int)tile_offsets[tile0 + c] + chunk_base[(int64_t)blockIdx.x * max_tiles_x + c];
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) {
+      const int t = s_cnt[k * max_tiles_x + c];
+      s_cnt[k * max_tiles_x + c] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  int32_t* base = s_cnt + w * max_tiles_x;
+  uint32_t* bitmap = bitmap_all + w * max_tiles_x;
   const unsigned lt = lanemask_lt();
-  for (int step = w_begin; step < w_end; step += 32) {
-    const int rec = step + lane;
-    const bool valid = rec < w_end;
-    int x0 = 1 << 30, x1 = -1;
-    uint32_t slot = 0u;
-    if (valid) {
-      slot = rec_slots[rec];
-      const uint2 r = rect[slot];
-      x0 = r.x & 0xFFFF;
-      x1 = r.x >> 16;
-      for (int c = x0; c <= x1; ++c) atomicOr(&bitmap[c], 1u << lane);
+#pragma unroll
+  for (int k = 0; k < kPerLane; ++k) {
+    const int x0 = xr[k] & 0xFFFF, x1 = xr[k] >> 16;
+    for (int c = x0; c <= x1; ++c) atomicOr(&bitmap[c], 1u << lane);
+    __syncwarp();
+    for (int c = x0; c <= x1; ++c) {
+      const int64_t pos = (int64_t)base[c] + __popc(bitmap[c] & lt);
+      if (pos < capacity) tile_slots[pos] = slot[k];
     }
     __syncwarp();
-    if (valid) {
-      for (int c = x0; c <= x1; ++c) {
-        const int64_t pos = (int64_t)base[c] + __popc(bitmap[c] & lt);
-        if (pos < capacity) tile_slots[pos] = slot;
-      }
-    }
-    __syncwarp();
-    const int lo = __reduce_min_sync(kFull, x0), hi = __reduce_max_sync(kFull, x1);
+    const int lo = __reduce_min_sync(kFull, x1 >= x0 ? x0 : (1 << 30));
+    const int hi = __reduce_max_sync(kFull, x1 >= x0 ? x1 : -1);
     for (int c = lo + lane; c <= hi; c += 32) {
       const uint32_t m = bitmap[c];
       if (m != 0u) {
@@ -241,23 +342,32 @@ void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const
       sentinel_row, overflow);
 }
 
-size_t row_counts_smem(int max_tiles_x) { return sizeof(int32_t) * kWarps * max_tiles_x; }
-size_t row_expand_smem(int max_tiles_x) { return 2 * sizeof(int32_t) * kWarps * max_tiles_x; }
+size_t chunk_counts_smem(int max_tiles_x) { return sizeof(int32_t) * kWarps * max_tiles_x; }
+size_t chunk_expand_smem(int max_tiles_x) { return 2 * sizeof(int32_t) * kWarps * max_tiles_x; }
 
 void configure_bin_kernels() {
-  cudaFuncSetAttribute(k_row_counts, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)row_counts_smem(kMaxTilesX));
-  cudaFuncSetAttribute(k_row_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)row_expand_smem(kMaxTilesX));
+  cudaFuncSetAttribute(k_chunk_counts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)chunk_counts_smem(kMaxTilesX));
+  cudaFuncSetAttribute(k_chunk_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)chunk_expand_smem(kMaxTilesX));
 }
 
-void launch_row_counts(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+int64_t max_row_chunks(int64_t records, int total_rows) { return records / kChunk + total_rows + 1; }
+
+void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
                        const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
-                       int32_t* warp_base, int32_t* tile_counts, cudaStream_t stream) {
+                       int64_t max_chunks, int4* chunks, int32_t* n_chunks,
+                       int32_t* chunk_counts, int32_t* chunk_base, int32_t* tile_counts,
+                       cudaStream_t stream) {
   if (total_rows <= 0) return;
   count_launch();
-  k_row_counts<<<total_rows, kWarps * 32, row_counts_smem(max_tiles_x), stream>>>(
-      row_ranges, rec_slots, rect, views, n_views, max_tiles_x, warp_base, tile_counts);
+  k_row_chunks<<<1, 1024, 0, stream>>>(row_ranges, total_rows, (int)max_chunks, chunks, n_chunks);
+  count_launch();
+  k_chunk_counts<<<(unsigned)max_chunks, kWarps * 32, chunk_counts_smem(max_tiles_x), stream>>>(
+      chunks, n_chunks, rec_slots, rect, views, n_views, max_tiles_x, chunk_counts);
+  count_launch();
+  k_row_tiles<<<total_rows, 256, 0, stream>>>(chunks, n_chunks, views, n_views, max_tiles_x,
+                                              chunk_counts, chunk_base, tile_counts);
 }
 
 void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, int64_t n_tiles,
@@ -269,14 +379,15 @@ void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, i
       counts, offsets, n_tiles, capacity, ranges, overflow);
 }
 
-void launch_row_expand(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
-                       const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
-                       const int32_t* warp_base, const int64_t* tile_offsets, int64_t capacity,
-                       uint32_t* tile_slots, cudaStream_t stream) {
-  if (total_rows <= 0) return;
+void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint32_t* rec_slots,
+                         const uint2* rect, const ViewDesc* views, int n_views, int max_tiles_x,
+                         int64_t max_chunks, const int32_t* chunk_base,
+                         const int64_t* tile_offsets, int64_t capacity, uint32_t* tile_slots,
+                         cudaStream_t stream) {
+  if (max_chunks <= 0) return;
   count_launch();
-  k_row_expand<<<total_rows, kWarps * 32, row_expand_smem(max_tiles_x), stream>>>(
-      row_ranges, rec_slots, rect, views, n_views, max_tiles_x, warp_base, tile_offsets,
+  k_chunk_expand<<<(unsigned)max_chunks, kWarps * 32, chunk_expand_smem(max_tiles_x), stream>>>(
+      chunks, n_chunks, rec_slots, rect, views, n_views, max_tiles_x, chunk_base, tile_offsets,
       capacity, tile_slots);
 }
 

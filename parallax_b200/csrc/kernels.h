@@ -71,16 +71,22 @@ void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const
                       const uint2* rect, const ViewDesc* views, int64_t slot_stride, int64_t n,
                       uint32_t* keys, uint32_t* vals, int64_t capacity, uint32_t sentinel_row,
                       int32_t* overflow, cudaStream_t stream);
-void launch_row_counts(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+// Upper bound on the number of row chunks for `records` records.
+int64_t max_row_chunks(int64_t records, int total_rows);
+// Chunk table, per-chunk column counts, per-chunk bases and tile lengths.
+void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
                        const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
-                       int32_t* warp_base, int32_t* tile_counts, cudaStream_t stream);
+                       int64_t max_chunks, int4* chunks, int32_t* n_chunks,
+                       int32_t* chunk_counts, int32_t* chunk_base, int32_t* tile_counts,
+                       cudaStream_t stream);
 void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, int64_t n_tiles,
                                 int64_t capacity, int2* ranges, int32_t* overflow,
                                 cudaStream_t stream);
-void launch_row_expand(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
-                       const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
-                       const int32_t* warp_base, const int64_t* tile_offsets, int64_t capacity,
-                       uint32_t* tile_slots, cudaStream_t stream);
+void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint32_t* rec_slots,
+                         const uint2* rect, const ViewDesc* views, int n_views, int max_tiles_x,
+                         int64_t max_chunks, const int32_t* chunk_base,
+                         const int64_t* tile_offsets, int64_t capacity, uint32_t* tile_slots,
+                         cudaStream_t stream);
 
 // raster.cu
 void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,

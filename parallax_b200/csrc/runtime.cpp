@@ -120,8 +120,7 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   tile_counts.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
   tile_offsets.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
   row_ranges.reserve(static_cast<size_t>(std::max(batch.total_rows, 1)));
-  warp_base.reserve(static_cast<size_t>(std::max(batch.total_rows, 1)) * 8 *
-                    static_cast<size_t>(std::max(batch.max_tiles_x, 1)));
+  n_chunks.reserve(1);
   d_total_records.reserve(1);
   loss_sums.reserve(static_cast<size_t>(2 * std::max(V, 1)));
   loss_per_view.reserve(static_cast<size_t>(std::max(V, 1)));
@@ -154,12 +153,24 @@ void Frame::reserve_records(int64_t capacity) {
   rec_keys_alt.reserve(cap);
   rec_vals_alt.reserve(cap);
   record_capacity = static_cast<int64_t>(cap);
+  ensure_chunks();
   const size_t rec_hist = radix_hist_entries(record_capacity, 0, 9);
   if (hist.capacity() < rec_hist) {
     hist.reserve(rec_hist);
     hist_scanned.reserve(rec_hist);
   }
   ensure_scan_scratch(static_cast<int64_t>(hist.capacity()));
+}
+
+void Frame::ensure_chunks() {
+  const int64_t need = max_row_chunks(std::max<int64_t>(record_capacity, 1), batch.total_rows);
+  const size_t per = static_cast<size_t>(std::max(batch.max_tiles_x, 1));
+  if (need > max_chunks || chunk_counts.capacity() < static_cast<size_t>(need) * per) {
+    chunks.reserve(static_cast<size_t>(need));
+    chunk_counts.reserve(static_cast<size_t>(need) * per);
+    chunk_base.reserve(static_cast<size_t>(need) * per);
+    max_chunks = need;
+  }
 }
 
 void Frame::project(const float* params, cudaStream_t stream, bool want_debug) {
@@ -220,9 +231,11 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   PXS_CUDA(cudaMemsetAsync(row_ranges.get(), 0, sizeof(int2) * std::max(batch.total_rows, 1),
                            stream));
   launch_tile_ranges(rk, n_rec, n_dev, n_rows, row_ranges.get(), stream);
-  // 4. tile lengths per row, their offsets, then the lists themselves
-  launch_row_counts(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
-                    batch.max_tiles_x, warp_base.get(), tile_counts.get(), stream);
+  // 4. tile lengths from chunked rows, their offsets, then the lists themselves
+  ensure_chunks();
+  launch_tile_lists(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
+                    batch.max_tiles_x, max_chunks, chunks.get(), n_chunks.get(),
+                    chunk_counts.get(), chunk_base.get(), tile_counts.get(), stream);
   exclusive_scan_i32_to_i64(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
                             d_total_pairs.get(), scan_, stream);
   PXS_CUDA(cudaGetLastError());
@@ -236,9 +249,9 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   }
   launch_ranges_from_offsets(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
                              pair_capacity, ranges.get(), overflow.get(), stream);
-  launch_row_expand(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
-                    batch.max_tiles_x, warp_base.get(), tile_offsets.get(), pair_capacity,
-                    tile_slots.get(), stream);
+  launch_chunk_expand(chunks.get(), n_chunks.get(), rv, rect.get(), d_views.get(), V,
+                      batch.max_tiles_x, max_chunks, chunk_base.get(), tile_offsets.get(),
+                      pair_capacity, tile_slots.get(), stream);
   sorted_pair_vals = tile_slots.get();
   PXS_CUDA(cudaGetLastError());
   return K;

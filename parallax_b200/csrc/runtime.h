@@ -141,7 +141,9 @@ class Frame {
   DeviceArray<int64_t> pair_offsets, d_total_pairs, d_total_records;
   DeviceArray<uint32_t> rec_keys, rec_vals, rec_keys_alt, rec_vals_alt;  // tile-row records
   DeviceArray<int2> row_ranges;
-  DeviceArray<int32_t> warp_base, tile_counts;
+  DeviceArray<int32_t> tile_counts, chunk_counts, chunk_base, n_chunks;
+  DeviceArray<int4> chunks;
+  int64_t max_chunks = 0;
   DeviceArray<int64_t> tile_offsets;
   DeviceArray<uint32_t> tile_slots;  // per-tile key lists (pair_capacity)
   DeviceArray<uint32_t> hist, hist_scanned;
@@ -160,6 +162,7 @@ class Frame {
 
  private:
   void ensure_scan_scratch(int64_t n);
+  void ensure_chunks();
   ScanScratch scan_;
   int64_t scan_capacity_ = 0;
   bool configured_ = false;
