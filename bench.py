@@ -124,16 +124,30 @@ def load_cpu_baseline():
     ref = os.path.join(ROOT, "oracle", "_ref", "libpxref_fast.so")
     if os.path.exists(ref):
         lib = ct.CDLL(ref)
-        lib.ref_project.restype = ct.c_int
-        lib.ref_render_and_accumulate.restype = ct.c_float
+        view = [_vp, ct.c_int, ct.c_int, ct.c_int, _vp, ct.c_int, ct.c_int, _vp, _vp, _vp]
+        _sig(lib.ref_project, ct.c_int, view + [_vp])
+        _sig(lib.ref_render, None, view + [_vp, _vp])
+        _sig(lib.ref_render_and_accumulate, ct.c_float,
+             view + [_vp, ct.c_float, _vp, _vp, _vp])
         return "reference", lib
     port = os.path.join(ROOT, "oracle", "libpxo.so")
     if not os.path.exists(port):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
     lib = ct.CDLL(port)
-    lib.pxo_project_f32.restype = ct.c_int32
-    lib.pxo_render_and_accumulate_f32.restype = ct.c_float
+    i32 = ct.c_int32
+    _sig(lib.pxo_project_f32, i32, [_vp, i32, i32, i32, _vp, _vp, _vp])
+    _sig(lib.pxo_rasterize_f32, None, [_vp, i32, _vp, _vp, _vp, _vp])
+    _sig(lib.pxo_render_and_accumulate_f32, ct.c_float,
+         [_vp, i32, i32, i32, _vp, _vp, _vp, ct.c_float, _vp, _vp, _vp])
     return "port", lib
+
+
+_vp = ct.c_void_p
+
+
+def _sig(fn, restype, argtypes):
+    fn.restype = restype
+    fn.argtypes = argtypes
 
 
 class CpuSample:
