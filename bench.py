@@ -52,6 +52,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", default="c4")
+    p.add_argument("--views", type=int, default=0,
+                   help="views per step (default: the workload's); a smaller case for profiling")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -296,7 +298,7 @@ def run_ours(args):
     from parallax_b200.scenes import WORKLOADS, workload_scene
 
     w = WORKLOADS[args.workload]
-    V = w["views_per_step"]
+    V = args.views or w["views_per_step"]
     truth, start, views = workload_scene(args.workload)
     P = px.param_count(start.rest_per_channel)
     N = start.count

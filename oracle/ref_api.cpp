@@ -21,6 +21,14 @@
 #include "parallax/splat/SplatTrainer.h"
 #include "pxs.h"
 
+#ifdef PXREF_SHIM
+#include <algorithm>
+#include <limits>
+#include <stdexcept>
+
+#include "CudaSplatTrainer.h"
+#endif
+
 using namespace parallax;
 
 namespace {
@@ -169,6 +177,20 @@ void addGradients(const SplatGradients& g, int rest, float* grads, float* screen
     screen[i] += g.screen_gradient[i];
     visible[i] += g.visible_count[i];
   }
+}
+
+std::vector<SplatTrainingView> toViews(int n_views, const double* K, const int32_t* sizes,
+                                       const double* R, const double* t,
+                                       const float* const* images) {
+  std::vector<SplatTrainingView> views;
+  for (int v = 0; v < n_views; ++v) {
+    SplatTrainingView tv;
+    tv.view = toView(K + 4 * v, sizes[2 * v], sizes[2 * v + 1], R + 9 * v, t + 3 * v);
+    const size_t values = static_cast<size_t>(sizes[2 * v]) * sizes[2 * v + 1] * 3;
+    tv.image.assign(images[v], images[v] + values);
+    views.push_back(std::move(tv));
+  }
+  return views;
 }
 
 struct RefTrainer {
@@ -326,18 +348,11 @@ void* ref_trainer_create(const float* params, int n, int rest, int cloud_sh, int
                          const double* K, const int32_t* sizes, const double* R,
                          const double* t, const float* const* images,
                          const pxs_train_config* config) {
-  std::vector<SplatTrainingView> views;
-  for (int v = 0; v < n_views; ++v) {
-    SplatTrainingView tv;
-    tv.view = toView(K + 4 * v, sizes[2 * v], sizes[2 * v + 1], R + 9 * v, t + 3 * v);
-    const size_t values = static_cast<size_t>(sizes[2 * v]) * sizes[2 * v + 1] * 3;
-    tv.image.assign(images[v], images[v] + values);
-    views.push_back(std::move(tv));
-  }
   auto* holder = new RefTrainer;
   holder->rest = rest;
-  holder->trainer = std::make_unique<SplatTrainer>(toCloud(params, n, rest, cloud_sh),
-                                                   std::move(views), toConfig(config));
+  holder->trainer = std::make_unique<SplatTrainer>(
+      toCloud(params, n, rest, cloud_sh), toViews(n_views, K, sizes, R, t, images),
+      toConfig(config));
   return holder;
 }
 
@@ -420,5 +435,96 @@ void ref_config_defaults(pxs_train_config* c) {
   c->max_gaussians = d.max_gaussians;
   c->seed = d.seed;
 }
+
+#ifdef PXREF_SHIM
+// ------------------------------------------- the drop-in shim, in the engine
+// Built into oracle/_ref/libpxshim.so together with
+// parallax_b200/shim/CudaSplatTrainer.cpp and linked against libpxs.so: the
+// reference's own SplatTrainer and the engine signatures, run on the GPU core.
+
+int ref_shim_availability(int32_t* available, char* name, int name_len, char* reason,
+                          int reason_len) {
+  const SplatGpuAvailability a = splatGpuAvailability();
+  *available = a.available ? 1 : 0;
+  if (name != nullptr && name_len > 0) {
+    std::strncpy(name, a.device_name.c_str(), static_cast<size_t>(name_len) - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (reason != nullptr && reason_len > 0) {
+    std::strncpy(reason, a.reason.c_str(), static_cast<size_t>(reason_len) - 1);
+    reason[reason_len - 1] = '\0';
+  }
+  return 0;
+}
+
+// SplatBackend::renderAndAccumulate of makeCudaSplatBackend(), same arguments
+// as ref_render_and_accumulate. Returns NaN when the backend fails.
+float ref_shim_render_and_accumulate(const float* params, int n, int rest, int cloud_sh,
+                                     const double* K, int width, int height, const double* R,
+                                     const double* t, const pxs_raster_options* opt,
+                                     const float* target, float ssim_weight, float* grads,
+                                     float* screen, int32_t* visible) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const SplatView view = toView(K, width, height, R, t);
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  std::vector<float> tgt(target, target + values);
+  SplatGradients g;  // left empty: the backend sizes it, as the CPU one does
+  std::unique_ptr<SplatBackend> backend = makeCudaSplatBackend(0);
+  if (backend == nullptr) return std::numeric_limits<float>::quiet_NaN();
+  try {
+    const float loss =
+        backend->renderAndAccumulate(cloud, view, toOptions(opt), tgt, ssim_weight, &g);
+    addGradients(g, rest, grads, screen, visible);
+    return loss;
+  } catch (const std::exception&) {
+    return std::numeric_limits<float>::quiet_NaN();
+  }
+}
+
+// The reference's SplatTrainer driving makeCudaSplatBackend(); the other
+// ref_trainer_* calls work on the handle.
+void* ref_shim_trainer_create(const float* params, int n, int rest, int cloud_sh, int n_views,
+                              const double* K, const int32_t* sizes, const double* R,
+                              const double* t, const float* const* images,
+                              const pxs_train_config* config) {
+  std::unique_ptr<SplatBackend> backend = makeCudaSplatBackend(0);
+  if (backend == nullptr) return nullptr;
+  auto* holder = new RefTrainer;
+  holder->rest = rest;
+  holder->trainer = std::make_unique<SplatTrainer>(
+      toCloud(params, n, rest, cloud_sh), toViews(n_views, K, sizes, R, t, images),
+      toConfig(config), std::move(backend));
+  return holder;
+}
+
+// trainSplatsOnGpu through the engine signature. `params` has room for
+// max(n, config->max_gaussians) gaussians; on success it receives the trained
+// cloud with stride *count. The callback cancels once `cancel_at` is reached
+// (0 never). Returns 1 on success, 0 with the message in `error`.
+int ref_shim_train_splats_on_gpu(float* params, int n, int rest, int cloud_sh, int n_views,
+                                 const double* K, const int32_t* sizes, const double* R,
+                                 const double* t, const float* const* images,
+                                 const pxs_train_config* config, int cancel_at, int* count,
+                                 int* sh_degree, int* last_seen, char* error, int error_len) {
+  GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  std::string why;
+  int seen = 0;
+  const SplatTrainingCallback callback = [&](const SplatTrainingProgress& p) {
+    seen = p.iteration;
+    return cancel_at <= 0 || p.iteration < cancel_at;
+  };
+  const bool ok = trainSplatsOnGpu(&cloud, toViews(n_views, K, sizes, R, t, images),
+                                   toConfig(config), callback, &why);
+  if (last_seen != nullptr) *last_seen = seen;
+  if (error != nullptr && error_len > 0) {
+    std::strncpy(error, why.c_str(), static_cast<size_t>(error_len) - 1);
+    error[error_len - 1] = '\0';
+  }
+  if (!ok) return 0;
+  *count = fromCloud(cloud, rest, params, std::max(n, config->max_gaussians));
+  *sh_degree = cloud.sh_degree;
+  return 1;
+}
+#endif  // PXREF_SHIM
 
 }  // extern "C"

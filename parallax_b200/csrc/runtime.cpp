@@ -134,6 +134,9 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   ensure_scan_scratch(std::max<int64_t>(std::max<int64_t>(static_cast<int64_t>(slots),
                                                           static_cast<int64_t>(hist.capacity())),
                                         batch.total_tiles));
+  // the chunk table depends on the rows as well as on the record capacity; size
+  // it here, before any stream capture of the binning stage
+  if (record_capacity > 0) ensure_chunks();
 }
 
 void Frame::reserve_pairs(int64_t capacity) {

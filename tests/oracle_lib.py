@@ -68,14 +68,19 @@ def pxo() -> ct.CDLL:
 
 
 def ref_available(kind: str = "ieee") -> bool:
-    return os.path.exists(os.path.join(ORACLE_DIR, "_ref", f"libpxref_{kind}.so"))
+    return os.path.exists(ref_path(kind))
+
+
+def ref_path(kind: str = "ieee") -> str:
+    name = "libpxshim.so" if kind == "shim" else f"libpxref_{kind}.so"
+    return os.path.join(ORACLE_DIR, "_ref", name)
 
 
 def ref(kind: str = "ieee") -> ct.CDLL:
-    """The reference's own code: kind 'ieee' (parity) or 'fast' (its release flags)."""
+    """The reference's own code: kind 'ieee' (parity), 'fast' (its release
+    flags) or 'shim' (the IEEE build with the drop-in shim over libpxs.so)."""
     if kind not in _REF:
-        path = os.path.join(ORACLE_DIR, "_ref", f"libpxref_{kind}.so")
-        lib = ct.CDLL(path)
+        lib = ct.CDLL(ref_path(kind))
         lib.ref_project.restype = ct.c_int
         lib.ref_photometric_loss.restype = ct.c_float
         lib.ref_mean_ssim.restype = ct.c_float
@@ -91,6 +96,15 @@ def ref(kind: str = "ieee") -> ct.CDLL:
         lib.ref_trainer_download.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int]
         lib.ref_trainer_finish.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]
         lib.ref_trainer_destroy.argtypes = [ct.c_void_p]
+        if kind == "shim":
+            lib.ref_shim_trainer_create.restype = ct.c_void_p
+            lib.ref_shim_trainer_create.argtypes = lib.ref_trainer_create.argtypes
+            lib.ref_shim_render_and_accumulate.restype = ct.c_float
+            lib.ref_shim_availability.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_int,
+                                                  ct.c_char_p, ct.c_int]
+            lib.ref_shim_train_splats_on_gpu.argtypes = (
+                [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int] + [ct.c_void_p] * 6
+                + [ct.c_int] + [ct.c_void_p] * 3 + [ct.c_char_p, ct.c_int])
         _REF[kind] = lib
     return _REF[kind]
 
@@ -526,7 +540,8 @@ class RefTrainer:
         self._images = [np.ascontiguousarray(im, dtype=np.float32) for im in images]
         ptrs = (ct.c_void_p * max(nv, 1))(*[im.ctypes.data for im in self._images])
         self.config = config
-        self.handle = self.lib.ref_trainer_create(
+        create = self.lib.ref_shim_trainer_create if kind == "shim" else self.lib.ref_trainer_create
+        self.handle = create(
             as_ptr(params), params.shape[1], rest, sh_degree, nv,
             as_ptr(K) if nv else None, as_ptr(sizes) if nv else None,
             as_ptr(R) if nv else None, as_ptr(t) if nv else None, ptrs, ct.byref(config))
