@@ -250,6 +250,41 @@ int pxs_adam_device(pxs_context* context, float* params, float* grads, float* m,
                     float beta1, float beta2, float epsilon, float correction1,
                     float correction2, int32_t zero_grads);
 
+/* ------------------------------------------------- allocation-free variant
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: a host framework whose caching allocator owns the GPU's memory and
+ * its budget (memory taken behind its back can push it out of memory), or a
+ * loop sharing the GPU with other streams, where the device-wide
+ * synchronisation of cudaFree would stall them. It also needs no context,
+ * whose buffers grow by allocation.
+ *
+ * The photometric loss of n_views images of width x height, on device
+ * buffers: rendered, target and dL_drgb hold n_views * height * width * 3
+ * floats (image after image, row-major RGB). It is pxs_photometric_loss per
+ * image, batched: per_view_loss[v] (device, n_views floats) gets image v's
+ * loss and `loss` (device, one float) their mean; dL_drgb, per_view_loss and
+ * loss may each be NULL. Work is queued on `stream` (a cudaStream_t; NULL is
+ * the default stream) and nothing waits for it.
+ *
+ * The kernel's scratch (per-image descriptors and sums) lives in a static
+ * array of PXS_STATIC_LOSS_SCRATCH_BYTES in device memory, which every GPU
+ * that loads this library holds until the process exits; so n_views is
+ * limited to PXS_STATIC_LOSS_MAX_VIEWS, and a larger count is rejected with
+ * PXS_ERR_INVALID. The call allocates no device memory and calls no
+ * allocating routine. The first call on each device (the current one) looks
+ * up the array's address and sets the kernel's shared-memory limit, once; make
+ * that first call before any stream capture. Every call on a device shares
+ * the one array: calls whose work overlaps on the GPU (two streams, two host
+ * threads) race and give wrong results, so order them (one stream, or
+ * events). Each call clears the sums it uses before the kernel runs.
+ * On failure the reason is written to `error` (may be NULL). */
+#define PXS_STATIC_LOSS_MAX_VIEWS 64
+#define PXS_STATIC_LOSS_SCRATCH_BYTES 16384
+int pxs_photometric_loss_static(const float* rendered, const float* target, int32_t width,
+                                int32_t height, int32_t n_views, float ssim_weight,
+                                float* dL_drgb, float* per_view_loss, float* loss,
+                                void* stream, char* error, size_t error_len);
+
 /* --------------------------------------------------------------- trainer
  * A device-resident SplatTrainer (SplatTrainer.h:132-161): the cloud, the
  * gradients, the Adam moments and the training images stay in device memory

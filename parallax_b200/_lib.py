@@ -67,6 +67,8 @@ def _declare(lib: ct.CDLL) -> None:
                                         ct.c_char_p, ct.c_size_t]),
         "pxs_densify_and_prune": (ct.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _f32, _i32,
                                              _vp, _vp, _vp, _vp, _vp]),
+        "pxs_photometric_loss_static": (ct.c_int, [_vp, _vp, _i32, _i32, _i32, _f32, _vp, _vp,
+                                                   _vp, _vp, ct.c_char_p, ct.c_size_t]),
         "pxs_synthetic_cloud": (ct.c_int, [ct.c_uint64, _i32, _i32, _f32, _vp]),
         "pxs_synthetic_cameras": (ct.c_int, [ct.c_uint64, _i32, _i32, ct.c_double, _i32, _i32,
                                              ct.c_double, _vp]),

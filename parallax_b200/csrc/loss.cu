@@ -11,8 +11,13 @@
 // Each blur pass is register-blocked: a thread loads a strip once and slides
 // the 11 taps along it. Sums run in the reference's tap order (fused
 // multiply-adds allowed); the scalar totals are accumulated in double.
+#include <cstdio>
+#include <exception>
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
+#include "runtime.h"
 
 namespace pxs {
 namespace {
@@ -294,3 +299,133 @@ void launch_loss(const float* rendered, const float* target, const ViewDesc* vie
 }
 
 }  // namespace pxs
+
+// ------------------------------------------------ allocation-free entry point
+//
+// pxs_photometric_loss_static serves callers that cannot allocate device
+// memory (a host framework whose caching allocator owns the GPU's memory, or
+// a loop that must not pay cudaFree's device-wide synchronisation). The loss
+// kernel's scratch -- the per-image descriptors it reads and the two double
+// sums per image it accumulates into -- lives here, in one file-scope array
+// that every GPU loading the library holds until the process exits. Its name
+// in host code stands in for the symbol only; the device address comes from
+// cudaGetSymbolAddress, looked up once per device on the first call there.
+// Every call shares the array and finds the previous call's contents in it:
+// the descriptors are rewritten and the sums cleared before each kernel runs,
+// and calls that overlap on the GPU race.
+
+namespace pxs {
+namespace {
+
+struct StaticLossScratch {
+  ViewDesc views[PXS_STATIC_LOSS_MAX_VIEWS];
+  double sums[2 * PXS_STATIC_LOSS_MAX_VIEWS];
+};
+static_assert(sizeof(StaticLossScratch) <= PXS_STATIC_LOSS_SCRATCH_BYTES,
+              "the static loss scratch does not hold its views");
+
+static __device__ __align__(256) unsigned char g_loss_scratch[PXS_STATIC_LOSS_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+StaticLossScratch* g_scratch_addr[kMaxDevices] = {};
+
+// Image v of a batch of same-sized images laid out one after another.
+__global__ void k_static_loss_views(StaticLossScratch* scratch, int width, int height,
+                                    int n_views) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_views) return;
+  ViewDesc d;
+  memset(&d, 0, sizeof(d));
+  d.cam.width = width;
+  d.cam.height = height;
+  d.pixel_offset = (int64_t)v * width * height;
+  d.target_offset = d.pixel_offset;
+  scratch->views[v] = d;
+}
+
+struct StaticError {
+  int status;
+  const char* what;
+};
+
+// The scratch's device address on the current device; the first call on a
+// device looks it up and raises the loss kernel's shared-memory limit.
+StaticLossScratch* static_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_addr[device] == nullptr) {
+    void* ptr = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&ptr, g_loss_scratch);
+    if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+    err = cudaFuncSetAttribute(k_loss, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(LossSmem));
+    if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+    g_scratch_addr[device] = static_cast<StaticLossScratch*>(ptr);
+  }
+  return g_scratch_addr[device];
+}
+
+int static_fail(int status, const char* what, char* error, size_t error_len) {
+  if (error != nullptr && error_len > 0) std::snprintf(error, error_len, "%s", what);
+  return status;
+}
+
+}  // namespace
+}  // namespace pxs
+
+extern "C" int pxs_photometric_loss_static(const float* rendered, const float* target,
+                                           int32_t width, int32_t height, int32_t n_views,
+                                           float ssim_weight, float* dL_drgb,
+                                           float* per_view_loss, float* loss, void* stream,
+                                           char* error, size_t error_len) {
+  using namespace pxs;
+  char why[160];
+  if (width < 0 || height < 0 || n_views < 0)
+    return static_fail(PXS_ERR_INVALID, "negative image size or count", error, error_len);
+  if (n_views > PXS_STATIC_LOSS_MAX_VIEWS) {
+    std::snprintf(why, sizeof(why),
+                  "n_views = %d exceeds the static scratch limit of %d images per call",
+                  (int)n_views, PXS_STATIC_LOSS_MAX_VIEWS);
+    return static_fail(PXS_ERR_INVALID, why, error, error_len);
+  }
+  const bool empty = n_views == 0 || width == 0 || height == 0;
+  if (!empty && (rendered == nullptr || target == nullptr))
+    return static_fail(PXS_ERR_INVALID, "image is null", error, error_len);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  try {
+    if (empty) {  // nothing to score: every loss is 0
+      if (loss != nullptr) {
+        const cudaError_t err = cudaMemsetAsync(loss, 0, sizeof(float), s);
+        if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+      }
+      if (per_view_loss != nullptr && n_views > 0) {
+        const cudaError_t err = cudaMemsetAsync(per_view_loss, 0, sizeof(float) * n_views, s);
+        if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+      }
+      return PXS_OK;
+    }
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+    if (device < 0 || device >= kMaxDevices)
+      throw StaticError{PXS_ERR_UNAVAILABLE, "device ordinal beyond the supported range"};
+    StaticLossScratch* scratch = static_scratch(device);
+    cudaGetLastError();  // an earlier, unrelated failure is not this call's
+    count_launch();
+    k_static_loss_views<<<(n_views + 63) / 64, 64, 0, s>>>(scratch, width, height, n_views);
+    LossParams lp;
+    ssim_kernel_weights(lp.kernel);
+    lp.ssim_weight = ssim_weight;
+    lp.mode = 0;
+    // launch_loss clears scratch->sums on `s` before the kernel adds into them.
+    launch_loss(rendered, target, scratch->views, n_views, width, height, lp, dL_drgb,
+                scratch->sums, per_view_loss, loss, s);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) throw StaticError{PXS_ERR_CUDA, cudaGetErrorString(err)};
+    return PXS_OK;
+  } catch (const StaticError& e) {
+    return static_fail(e.status, e.what, error, error_len);
+  } catch (const std::exception& e) {
+    return static_fail(PXS_ERR_CUDA, e.what(), error, error_len);
+  }
+}
