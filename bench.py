@@ -366,6 +366,12 @@ def run_ours(args):
         step_counter[0] += 1
         batch_step(step_counter[0])
 
+    # the autotuner picks pixels per thread for compositing and its adjoint
+    fpx, bpx = ct.c_int32(), ct.c_int32()
+    ids0 = (ct.c_int32 * V)(*ids_for(0))
+    trainer._check(lib.pxs_trainer_autotune(trainer.handle, V, ids0, ct.byref(fpx),
+                                            ct.byref(bpx)))
+
     # warm-up: capture the graph, then once more with stage timing on
     for _ in range(max(args.warmup, 3)):
         next_batch(0)
@@ -480,7 +486,8 @@ def run_ours(args):
                                "pool, fwd+L1/SSIM+bwd+Adam",
                    "gaussians": N, "views_per_step": V, "width": w["width"],
                    "height": w["height"], "parallelism": f"dp{world} over views",
-                   "l2": "inputs larger than L2 (no flush)"},
+                   "l2": "inputs larger than L2 (no flush)",
+                   "pixels_per_thread": {"forward": fpx.value, "backward": bpx.value}},
         "plain": {"ms_per_step": ms_plain,
                   "value": world * 1000.0 / ms_plain if ms_plain else None,
                   "batched_over_plain": (ms_plain / ms_batched) if ms_plain else None,

@@ -329,6 +329,22 @@ int pxs_trainer_step_views(pxs_trainer* trainer, int32_t n_views, const int32_t*
 int pxs_trainer_render(pxs_trainer* trainer, const pxs_camera* camera,
                        const pxs_raster_options* options, float* rgb, float* transmittance);
 
+/* Pixels per thread of the compositing kernel and of its adjoint: 1, 2 or 4
+ * each (0 keeps the current value; anything else is PXS_ERR_INVALID). The
+ * setting is process-wide and read at launch; a trainer re-captures its step
+ * graph after a change. The results do not depend on it beyond the order in
+ * which the adjoint sums gradients. */
+int pxs_set_raster_config(int32_t forward_px, int32_t backward_px);
+int pxs_get_raster_config(int32_t* forward_px, int32_t* backward_px);
+
+/* The autotuner: times the compositing kernel and its adjoint with 1, 2 and
+ * 4 pixels per thread on the batch of `view_ids` (NULL: the first n_views
+ * views) and keeps the fastest of each (written to forward_px / backward_px,
+ * either may be NULL). The schedule, the cloud and its gradients are not
+ * changed. */
+int pxs_trainer_autotune(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
+                         int32_t* forward_px, int32_t* backward_px);
+
 /* Measures this device's FP32 FMA throughput (TFLOP/s) with a microkernel:
  * the roofline denominator of the FP32-bound compositing kernels. */
 int pxs_measure_fp32_peak(int32_t device, float* tflops);

@@ -233,6 +233,23 @@ void pxs_context_destroy(pxs_context* ctx) {
   delete ctx;
 }
 
+int pxs_set_raster_config(int32_t forward_px, int32_t backward_px) {
+  auto ok = [](int32_t v) { return v == 0 || v == 1 || v == 2 || v == 4; };
+  if (!ok(forward_px) || !ok(backward_px)) return PXS_ERR_INVALID;
+  pxs::RasterConfig& rc = pxs::raster_config();
+  if (forward_px) rc.forward_px = forward_px;
+  if (backward_px) rc.backward_px = backward_px;
+  ++rc.generation;
+  return PXS_OK;
+}
+
+int pxs_get_raster_config(int32_t* forward_px, int32_t* backward_px) {
+  const pxs::RasterConfig& rc = pxs::raster_config();
+  if (forward_px) *forward_px = rc.forward_px;
+  if (backward_px) *backward_px = rc.backward_px;
+  return PXS_OK;
+}
+
 const char* pxs_context_last_error(const pxs_context* ctx) {
   return ctx == nullptr ? "context is null" : ctx->error.c_str();
 }

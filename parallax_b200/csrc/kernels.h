@@ -89,6 +89,15 @@ void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint
                          cudaStream_t stream);
 
 // raster.cu
+// Pixels per thread of the compositing kernels (1, 2 or 4; TileGeom in
+// raster_common.cuh). Read at launch; set before a graph is captured.
+struct RasterConfig {
+  int forward_px = 2;
+  int backward_px = 2;
+  int generation = 0;  // bumped on every change; captured graphs compare it
+};
+RasterConfig& raster_config();
+
 void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,

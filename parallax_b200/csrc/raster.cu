@@ -1,6 +1,7 @@
 // raster.cu -- front-to-back alpha compositing.
 //
-// One CTA per (view, 16x16 tile), one thread per pixel. Each tile's key list
+// One CTA per (view, 16x16 tile), PX pixels per thread (1, 2 or 4, chosen by
+// the raster configuration; raster_common.cuh). Each tile's key list
 // is walked in batches of 256 entries staged through shared memory; the CTA
 // stops as soon as every pixel has reached the transmittance cutoff
 // (__syncthreads_and). Arithmetic follows rasterizeSplats
@@ -13,86 +14,119 @@
 
 namespace pxs {
 
+RasterConfig& raster_config() {
+  static RasterConfig config;
+  return config;
+}
+
 // rasterizeSplats (SplatRaster.cpp:265-315). Writes rgb (+ T * background),
 // the final transmittance and, for the adjoint, one past the index of the
 // last entry that contributed (the `last` of SplatRaster.cpp:363-376).
-// With kCount it also counts the (pixel, entry) pairs the loop evaluates and
-// those that pass both alpha tests into counts[0] and counts[1].
-template <bool kCount>
-__global__ void __launch_bounds__(kTilePixels)
+// Each thread composites PX pixels of one column (TileGeom). With kCount it
+// also counts the (pixel, entry) pairs the loop evaluates and those that pass
+// both alpha tests into counts[0] and counts[1].
+template <bool kCount, int PX>
+__global__ void __launch_bounds__(TileGeom<PX>::kThreads)
     k_forward(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
               const float2* __restrict__ xy, const float4* __restrict__ conic_op,
               const float4* __restrict__ color, const ViewDesc* __restrict__ views, int n_views,
               float* __restrict__ rgb_out, float* __restrict__ T_out,
               int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts) {
+  constexpr int kThreads = TileGeom<PX>::kThreads;
   __shared__ float2 s_xy[kBatch];
   __shared__ float4 s_co[kBatch];
   __shared__ float4 s_col[kBatch];  // r, g, b, power floor
   __shared__ uint32_t s_mask[kBatch];
-  const TileInfo info = tile_info(views, n_views, ranges);
+  const TileInfo<PX> info = tile_info<PX>(views, n_views, ranges);
   const int warp = threadIdx.x >> 5;
-  const int tile_px = info.px - (info.px % kTile), tile_py = info.py - (info.py % kTile);
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha, cutoff = vd.transmittance_cutoff;
-  const float fx = (float)info.px + 0.5f, fy = (float)info.py + 0.5f;
-  float T = 1.f;
-  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
-  int last = info.range.x;
-  bool done = !info.inside;
+  const float fx = (float)info.px + 0.5f;
+  float fy[PX], T[PX], acc0[PX], acc1[PX], acc2[PX];
+  int last[PX];
+  bool done[PX];
+  bool all_done = true;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    fy[p] = (float)(info.py0 + 4 * p) + 0.5f;
+    T[p] = 1.f;
+    acc0[p] = acc1[p] = acc2[p] = 0.f;
+    last[p] = info.range.x;
+    done[p] = !(info.px < vd.cam.width && info.py0 + 4 * p < vd.cam.height);
+    all_done = all_done && done[p];
+  }
   unsigned long long evaluated = 0, contributing = 0;
   for (int base = info.range.x; base < info.range.y; base += kBatch) {
-    if (__syncthreads_and(done)) break;
-    const int idx = base + (int)threadIdx.x;
-    if (idx < info.range.y) {
-      const uint32_t slot = pair_slots[idx];
+    if (__syncthreads_and(all_done)) break;
+    const int n = min(kBatch, info.range.y - base);
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const uint32_t slot = pair_slots[base + i];
       const float4 co = conic_op[slot];
       const float2 mean = xy[slot];
       float4 c = color[slot];
       c.w = power_floor(co.w, min_alpha);
-      s_xy[threadIdx.x] = mean;
-      s_co[threadIdx.x] = co;
-      s_col[threadIdx.x] = c;
-      s_mask[threadIdx.x] = warp_mask(mean, co, c.w, tile_px, tile_py);
+      s_xy[i] = mean;
+      s_co[i] = co;
+      s_col[i] = c;
+      s_mask[i] = warp_mask<PX>(mean, co, c.w, info.tile_px, info.tile_py);
     }
     __syncthreads();
-    const int n = min(kBatch, info.range.y - base);
-    if (!done) {
+    if (!all_done) {
       for (int j = 0; j < n; ++j) {
         if (!((s_mask[j] >> warp) & 1u)) {  // the splat cannot reach this warp's pixels
-          if (kCount) ++evaluated;
+          if (kCount) {
+#pragma unroll
+            for (int p = 0; p < PX; ++p) evaluated += done[p] ? 0 : 1;
+          }
           continue;
         }
         const float2 m = s_xy[j];
         const float4 co = s_co[j];
-        const float dx = fx - m.x, dy = fy - m.y;
-        const float power = splat_power(co, dx, dy);
-        if (kCount) ++evaluated;
-        if (power > 0.f || power < s_col[j].w) continue;
-        float alpha = co.w * expf(power);
-        alpha = alpha < kMaxAlpha ? alpha : kMaxAlpha;
-        if (alpha < min_alpha) continue;
-        if (kCount) ++contributing;
-        const float4 c = s_col[j];
-        const float ta = T * alpha;
-        acc0 += ta * c.x;
-        acc1 += ta * c.y;
-        acc2 += ta * c.z;
-        T *= 1.f - alpha;
-        last = base + j + 1;
-        if (T < cutoff) {
-          done = true;
+        const float floor = s_col[j].w;
+        const float dx = fx - m.x;
+        bool now_done = true;
+#pragma unroll
+        for (int p = 0; p < PX; ++p) {
+          if (!done[p]) {
+            if (kCount) ++evaluated;
+            const float dy = fy[p] - m.y;
+            const float power = splat_power(co, dx, dy);
+            if (!(power > 0.f || power < floor)) {
+              float alpha = co.w * expf(power);
+              alpha = alpha < kMaxAlpha ? alpha : kMaxAlpha;
+              if (!(alpha < min_alpha)) {
+                if (kCount) ++contributing;
+                const float4 c = s_col[j];
+                const float ta = T[p] * alpha;
+                acc0[p] += ta * c.x;
+                acc1[p] += ta * c.y;
+                acc2[p] += ta * c.z;
+                T[p] *= 1.f - alpha;
+                last[p] = base + j + 1;
+                if (T[p] < cutoff) done[p] = true;
+              }
+            }
+          }
+          now_done = now_done && done[p];
+        }
+        if (now_done) {
+          all_done = true;
           break;
         }
       }
     }
   }
-  if (info.inside) {
-    const int64_t pixel = vd.pixel_offset + (int64_t)info.py * vd.cam.width + info.px;
-    rgb_out[pixel * 3 + 0] = acc0 + T * vd.background[0];
-    rgb_out[pixel * 3 + 1] = acc1 + T * vd.background[1];
-    rgb_out[pixel * 3 + 2] = acc2 + T * vd.background[2];
-    if (T_out != nullptr) T_out[pixel] = T;
-    last_out[pixel] = last;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    const int py = info.py0 + 4 * p;
+    if (info.px < vd.cam.width && py < vd.cam.height) {
+      const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
+      rgb_out[pixel * 3 + 0] = acc0[p] + T[p] * vd.background[0];
+      rgb_out[pixel * 3 + 1] = acc1[p] + T[p] * vd.background[1];
+      rgb_out[pixel * 3 + 2] = acc2[p] + T[p] * vd.background[2];
+      if (T_out != nullptr) T_out[pixel] = T[p];
+      last_out[pixel] = last[p];
+    }
   }
   if (kCount) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -106,19 +140,52 @@ __global__ void __launch_bounds__(kTilePixels)
   }
 }
 
+namespace {
+
+template <bool kCount, int PX>
+void forward_px(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                const float4* conic_op, const float4* color, const ViewDesc* views, int n_views,
+                int total_tiles, float* rgb, float* T, int32_t* last, cudaStream_t stream,
+                unsigned long long* counts) {
+  k_forward<kCount, PX><<<total_tiles, TileGeom<PX>::kThreads, 0, stream>>>(
+      ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts);
+}
+
+template <bool kCount>
+void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                      const float4* conic_op, const float4* color, const ViewDesc* views,
+                      int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
+                      cudaStream_t stream, unsigned long long* counts) {
+  switch (px) {
+    case 1:
+      forward_px<kCount, 1>(ranges, pair_slots, xy, conic_op, color, views, n_views,
+                            total_tiles, rgb, T, last, stream, counts);
+      break;
+    case 4:
+      forward_px<kCount, 4>(ranges, pair_slots, xy, conic_op, color, views, n_views,
+                            total_tiles, rgb, T, last, stream, counts);
+      break;
+    default:
+      forward_px<kCount, 2>(ranges, pair_slots, xy, conic_op, color, views, n_views,
+                            total_tiles, rgb, T, last, stream, counts);
+  }
+}
+
+}  // namespace
+
 void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
                     cudaStream_t stream, unsigned long long* counts) {
-  if (total_tiles > 0) {
-    count_launch();
-    if (counts != nullptr)
-      k_forward<true><<<total_tiles, kTilePixels, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts);
-    else
-      k_forward<false><<<total_tiles, kTilePixels, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, nullptr);
-  }
+  if (total_tiles <= 0) return;
+  count_launch();
+  const int px = raster_config().forward_px;
+  if (counts != nullptr)
+    forward_dispatch<true>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
+                           total_tiles, rgb, T, last, stream, counts);
+  else
+    forward_dispatch<false>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
+                            total_tiles, rgb, T, last, stream, nullptr);
 }
 
 }  // namespace pxs

@@ -61,13 +61,15 @@ __device__ __forceinline__ float warp_reduce10(const float (&v)[10], int lane, i
 
 }  // namespace
 
-__global__ void __launch_bounds__(kTilePixels)
+template <int PX>
+__global__ void __launch_bounds__(TileGeom<PX>::kThreads)
     k_backward(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                const float4* __restrict__ color, const ViewDesc* __restrict__ views,
                int n_views, const float* __restrict__ T_final,
                const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
                ScreenGrad* __restrict__ screen) {
+  constexpr int kThreads = TileGeom<PX>::kThreads;
   __shared__ uint32_t s_slot[kBatch];
   __shared__ float2 s_xy[kBatch];
   __shared__ float4 s_co[kBatch];
@@ -75,102 +77,119 @@ __global__ void __launch_bounds__(kTilePixels)
   __shared__ uint32_t s_mask[kBatch];
   __shared__ float s_acc[kBatch][12];
   __shared__ int s_hi;
-  const TileInfo info = tile_info(views, n_views, ranges);
+  const TileInfo<PX> info = tile_info<PX>(views, n_views, ranges);
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha;
-  const float fx = (float)info.px + 0.5f, fy = (float)info.py + 0.5f;
-  float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, final_T = 1.f;
-  int my_last = info.range.x;
-  if (info.inside) {
-    const int64_t pixel = vd.pixel_offset + (int64_t)info.py * vd.cam.width + info.px;
-    dLp0 = dL_drgb[pixel * 3 + 0];
-    dLp1 = dL_drgb[pixel * 3 + 1];
-    dLp2 = dL_drgb[pixel * 3 + 2];
-    final_T = T_final[pixel];
-    my_last = last_in[pixel];
+  const float fx = (float)info.px + 0.5f;
+  const float bg0 = vd.background[0], bg1 = vd.background[1], bg2 = vd.background[2];
+  // per pixel: dL/drgb, the final and the running transmittance, the suffix
+  // colour, the previous contributor's alpha and colour, the last contributor
+  float fy[PX], dLp0[PX], dLp1[PX], dLp2[PX], final_T[PX], T[PX], bg_term[PX];
+  float suffix0[PX], suffix1[PX], suffix2[PX], last_alpha[PX], lc0[PX], lc1[PX], lc2[PX];
+  int my_last[PX];
+  int thread_hi = info.range.x;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    const int py = info.py0 + 4 * p;
+    fy[p] = (float)py + 0.5f;
+    dLp0[p] = dLp1[p] = dLp2[p] = 0.f;
+    final_T[p] = 1.f;
+    my_last[p] = info.range.x;
+    if (info.px < vd.cam.width && py < vd.cam.height) {
+      const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
+      dLp0[p] = dL_drgb[pixel * 3 + 0];
+      dLp1[p] = dL_drgb[pixel * 3 + 1];
+      dLp2[p] = dL_drgb[pixel * 3 + 2];
+      final_T[p] = T_final[pixel];
+      my_last[p] = last_in[pixel];
+    }
+    T[p] = final_T[p];
+    bg_term[p] = final_T[p] * (bg0 * dLp0[p] + bg1 * dLp1[p] + bg2 * dLp2[p]);
+    suffix0[p] = suffix1[p] = suffix2[p] = 0.f;
+    last_alpha[p] = lc0[p] = lc1[p] = lc2[p] = 0.f;
+    thread_hi = max(thread_hi, my_last[p]);
   }
   const int lane = lane_id(), warp = warp_id();
-  const int tile_px = info.px - (info.px % kTile), tile_py = info.py - (info.py % kTile);
-  const int warp_hi = __reduce_max_sync(kFull, my_last);
+  const int warp_hi = __reduce_max_sync(kFull, thread_hi);
   if (threadIdx.x == 0) s_hi = info.range.x;
   __syncthreads();
   if (lane == 0 && warp_hi > info.range.x) atomicMax(&s_hi, warp_hi);
   __syncthreads();
   const int hi = s_hi;
-  float T = final_T;
-  float suffix0 = 0.f, suffix1 = 0.f, suffix2 = 0.f;
-  float last_alpha = 0.f, lc0 = 0.f, lc1 = 0.f, lc2 = 0.f;
-  const float background_term =
-      vd.background[0] * dLp0 + vd.background[1] * dLp1 + vd.background[2] * dLp2;
 
   for (int batch_end = hi; batch_end > info.range.x; batch_end -= kBatch) {
     const int batch_start = max(info.range.x, batch_end - kBatch);
     const int n = batch_end - batch_start;
     __syncthreads();
-    if ((int)threadIdx.x < n) {
-      const uint32_t slot = pair_slots[batch_start + threadIdx.x];
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const uint32_t slot = pair_slots[batch_start + i];
       const float4 co = conic_op[slot];
       const float2 mean = xy[slot];
       float4 c = color[slot];
       c.w = power_floor(co.w, min_alpha);
-      s_slot[threadIdx.x] = slot;
-      s_xy[threadIdx.x] = mean;
-      s_co[threadIdx.x] = co;
-      s_col[threadIdx.x] = c;
-      s_mask[threadIdx.x] = warp_mask(mean, co, c.w, tile_px, tile_py);
+      s_slot[i] = slot;
+      s_xy[i] = mean;
+      s_co[i] = co;
+      s_col[i] = c;
+      s_mask[i] = warp_mask<PX>(mean, co, c.w, info.tile_px, info.tile_py);
 #pragma unroll
-      for (int k = 0; k < 12; ++k) s_acc[threadIdx.x][k] = 0.f;
+      for (int k = 0; k < 12; ++k) s_acc[i][k] = 0.f;
     }
     __syncthreads();
     const int j_top = min(n, warp_hi - batch_start) - 1;  // warp-uniform
     for (int j = j_top; j >= 0; --j) {
       if (!((s_mask[j] >> warp) & 1u)) continue;  // the splat cannot reach this warp's pixels
       const int e = batch_start + j;
+      const float2 m = s_xy[j];
+      const float4 co = s_co[j];
+      const float4 c = s_col[j];
+      const float dx = fx - m.x;
       float v[10];
 #pragma unroll
       for (int k = 0; k < 10; ++k) v[k] = 0.f;
       bool contrib = false, touched = false;
-      if (e < my_last) {
-        const float2 m = s_xy[j];
-        const float4 co = s_co[j];
-        const float4 c = s_col[j];
-        const float dx = fx - m.x, dy = fy - m.y;
-        const float power = splat_power(co, dx, dy);
-        if (!(power > 0.f) && !(power < c.w)) {
-          const float gw = expf(power);
-          const float raw_alpha = __fmul_rn(co.w, gw);
-          const float alpha = raw_alpha < kMaxAlpha ? raw_alpha : kMaxAlpha;
-          if (!(alpha < min_alpha)) {
-            contrib = true;
-            const float inv = __fdividef(1.f, 1.f - alpha);
-            T *= inv;
-            const float weight = alpha * T;
-            v[6] = weight * dLp0;
-            v[7] = weight * dLp1;
-            v[8] = weight * dLp2;
-            suffix0 = last_alpha * lc0 + (1.f - last_alpha) * suffix0;
-            suffix1 = last_alpha * lc1 + (1.f - last_alpha) * suffix1;
-            suffix2 = last_alpha * lc2 + (1.f - last_alpha) * suffix2;
-            lc0 = c.x;
-            lc1 = c.y;
-            lc2 = c.z;
-            float dL_dalpha = ((c.x - suffix0) * dLp0 + (c.y - suffix1) * dLp1 +
-                               (c.z - suffix2) * dLp2) * T;
-            last_alpha = alpha;
-            dL_dalpha -= final_T * inv * background_term;
-            if (raw_alpha < kMaxAlpha) {  // the cap flattens the gradient
-              touched = true;
-              v[5] = gw * dL_dalpha;  // dopacity
-              const float dL_dweight = co.w * dL_dalpha;
-              const float gx = gw * dx, gy = gw * dy;
-              const float dm0 = dL_dweight * (-gx * co.x - gy * co.y);
-              const float dm1 = dL_dweight * (-gy * co.z - gx * co.y);
-              v[0] = -dm0;  // d(mean) = -d(delta)
-              v[1] = -dm1;
-              v[9] = sqrtf(dm0 * dm0 + dm1 * dm1);
-              v[2] = -0.5f * dL_dweight * gx * dx;
-              v[3] = -dL_dweight * gx * dy;
-              v[4] = -0.5f * dL_dweight * gy * dy;
+#pragma unroll
+      for (int p = 0; p < PX; ++p) {
+        if (e < my_last[p]) {
+          const float dy = fy[p] - m.y;
+          const float power = splat_power(co, dx, dy);
+          if (!(power > 0.f) && !(power < c.w)) {
+            const float gw = expf(power);
+            const float raw_alpha = __fmul_rn(co.w, gw);
+            const float alpha = raw_alpha < kMaxAlpha ? raw_alpha : kMaxAlpha;
+            if (!(alpha < min_alpha)) {
+              contrib = true;
+              const float inv = __fdividef(1.f, 1.f - alpha);
+              T[p] *= inv;
+              const float weight = alpha * T[p];
+              v[6] += weight * dLp0[p];
+              v[7] += weight * dLp1[p];
+              v[8] += weight * dLp2[p];
+              const float la = last_alpha[p];
+              suffix0[p] = la * lc0[p] + (1.f - la) * suffix0[p];
+              suffix1[p] = la * lc1[p] + (1.f - la) * suffix1[p];
+              suffix2[p] = la * lc2[p] + (1.f - la) * suffix2[p];
+              lc0[p] = c.x;
+              lc1[p] = c.y;
+              lc2[p] = c.z;
+              last_alpha[p] = alpha;
+              float dL_dalpha = ((c.x - suffix0[p]) * dLp0[p] + (c.y - suffix1[p]) * dLp1[p] +
+                                 (c.z - suffix2[p]) * dLp2[p]) * T[p];
+              dL_dalpha -= inv * bg_term[p];
+              if (raw_alpha < kMaxAlpha) {  // the cap flattens the gradient
+                touched = true;
+                v[5] += gw * dL_dalpha;  // dopacity
+                const float dL_dweight = co.w * dL_dalpha;
+                const float gx = gw * dx, gy = gw * dy;
+                const float dm0 = dL_dweight * (-gx * co.x - gy * co.y);
+                const float dm1 = dL_dweight * (-gy * co.z - gx * co.y);
+                v[0] -= dm0;  // d(mean) = -d(delta)
+                v[1] -= dm1;
+                v[9] += sqrtf(dm0 * dm0 + dm1 * dm1);
+                v[2] += -0.5f * dL_dweight * gx * dx;
+                v[3] += -dL_dweight * gx * dy;
+                v[4] += -0.5f * dL_dweight * gy * dy;
+              }
             }
           }
         }
@@ -188,10 +207,10 @@ __global__ void __launch_bounds__(kTilePixels)
       }
     }
     __syncthreads();
-    if ((int)threadIdx.x < n) {
-      const float* a = s_acc[threadIdx.x];
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const float* a = s_acc[i];
       if (a[11] != 0.f) {
-        float* dst = reinterpret_cast<float*>(&screen[s_slot[threadIdx.x]]);
+        float* dst = reinterpret_cast<float*>(&screen[s_slot[i]]);
         red_add_v4(dst + 0, a[0], a[1], a[2], a[3]);
         red_add_v4(dst + 4, a[4], a[5], a[6], a[7]);
         red_add_v4(dst + 8, a[8], a[9], a[10], 0.f);
@@ -200,15 +219,37 @@ __global__ void __launch_bounds__(kTilePixels)
   }
 }
 
+namespace {
+
+template <int PX>
+void backward_px(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                 const float4* conic_op, const float4* color, const ViewDesc* views, int n_views,
+                 int total_tiles, const float* T_final, const int32_t* last,
+                 const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream) {
+  k_backward<PX><<<total_tiles, TileGeom<PX>::kThreads, 0, stream>>>(
+      ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb, screen);
+}
+
+}  // namespace
+
 void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                      const float4* conic_op, const float4* color, const ViewDesc* views,
                      int n_views, int total_tiles, const float* T_final, const int32_t* last,
                      const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream) {
-  if (total_tiles > 0) {
-    count_launch();
-    k_backward<<<total_tiles, kTilePixels, 0, stream>>>(ranges, pair_slots, xy, conic_op, color,
-                                                        views, n_views, T_final, last, dL_drgb,
-                                                        screen);
+  if (total_tiles <= 0) return;
+  count_launch();
+  switch (raster_config().backward_px) {
+    case 1:
+      backward_px<1>(ranges, pair_slots, xy, conic_op, color, views, n_views, total_tiles,
+                     T_final, last, dL_drgb, screen, stream);
+      break;
+    case 4:
+      backward_px<4>(ranges, pair_slots, xy, conic_op, color, views, n_views, total_tiles,
+                     T_final, last, dL_drgb, screen, stream);
+      break;
+    default:
+      backward_px<2>(ranges, pair_slots, xy, conic_op, color, views, n_views, total_tiles,
+                     T_final, last, dL_drgb, screen, stream);
   }
 }
 

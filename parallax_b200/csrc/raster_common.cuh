@@ -11,53 +11,69 @@ namespace pxs {
 
 constexpr int kBatch = 256;
 
+// Pixels per thread. A warp covers an 8-wide block of 4*PX rows: lane l owns
+// column l%8 and rows l/8 + 4p (p < PX); warp w covers columns 8*(w%2) .. +8
+// and rows 4*PX*(w/2) .. +4*PX of the 16x16 tile. PX = 1 gives 8 warps of 8x4,
+// PX = 2 4 warps of 8x8, PX = 4 2 warps of 8x16. More pixels per thread share
+// each staged entry and each warp-level reduction among more pixels.
+template <int PX>
+struct TileGeom {
+  static constexpr int kThreads = kTilePixels / PX;
+  static constexpr int kWarps = kThreads / 32;
+  static constexpr int kBlockH = 4 * PX;
+};
+
+template <int PX>
 struct TileInfo {
   int view;
-  int px, py;  // this thread's pixel
-  bool inside;
+  int px;      // this thread's column
+  int py0;     // its first row; pixel p is at row py0 + 4p
+  int tile_px, tile_py;
   int2 range;
 };
 
-// Threads map to pixels by warps of 8x4 (warp w covers columns
-// 8*(w%2) .. +8 and rows 4*(w/2) .. +4 of the 16x16 tile), so a warp's pixels
-// are compact and can skip the entries whose footprint misses them.
-__device__ __forceinline__ TileInfo tile_info(const ViewDesc* __restrict__ views, int n_views,
-                                              const int2* __restrict__ ranges) {
-  TileInfo info;
+template <int PX>
+__device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ views,
+                                                  int n_views, const int2* __restrict__ ranges) {
+  TileInfo<PX> info;
   const int tile = blockIdx.x;
   info.view = view_of_tile(views, n_views, tile);
   const ViewDesc& vd = views[info.view];
   const int local = tile - vd.tile_offset;
   const int tx = local % vd.tiles_x, ty = local / vd.tiles_x;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  info.px = tx * kTile + (w & 1) * 8 + (lane & 7);
-  info.py = ty * kTile + (w >> 1) * 4 + (lane >> 3);
-  info.inside = info.px < vd.cam.width && info.py < vd.cam.height;
+  info.tile_px = tx * kTile;
+  info.tile_py = ty * kTile;
+  info.px = info.tile_px + (w & 1) * 8 + (lane & 7);
+  info.py0 = info.tile_py + (w >> 1) * TileGeom<PX>::kBlockH + (lane >> 3);
   info.range = ranges[tile];
   return info;
 }
 
-// Bit w is set when some pixel of warp w's 8x4 block may see this splat with
+// Bit w is set when some pixel of warp w's block may see this splat with
 // power >= `floor` (and so possibly alpha >= min_alpha). The region
 // {d : d^T A d <= -2 floor} of the conic A lies in the box
 // |dx| <= sqrt(-2 floor (A^-1)_xx), |dy| <= sqrt(-2 floor (A^-1)_yy); the box is
 // widened by 10% and half a pixel, which covers the rounding of the computed
 // power for any splat narrower than ~1000 px of standard deviation (wider ones
 // get every bit). No floor (min_alpha = 0) sets every bit.
+template <int PX>
 __device__ __forceinline__ uint32_t warp_mask(float2 mean, const float4& co, float floor,
                                               int tile_px, int tile_py) {
-  if (!(floor > -1e30f)) return 0xFFu;
+  constexpr uint32_t kAll = (1u << TileGeom<PX>::kWarps) - 1u;
+  if (!(floor > -1e30f)) return kAll;
   const float det = co.x * co.z - co.y * co.y;
-  if (!(det > 0.f)) return 0xFFu;
+  if (!(det > 0.f)) return kAll;
   const float k = -2.f * floor;
   const float ex = sqrtf(k * co.z / det) * 1.1f + 0.5f;
   const float ey = sqrtf(k * co.x / det) * 1.1f + 0.5f;
-  if (!(ex < 1e4f && ey < 1e4f)) return 0xFFu;
+  if (!(ex < 1e4f && ey < 1e4f)) return kAll;
   uint32_t m = 0u;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) {
+  for (int w = 0; w < TileGeom<PX>::kWarps; ++w) {
     const float x_lo = (float)(tile_px + (w & 1) * 8) + 0.5f, x_hi = x_lo + 7.f;
-    const float y_lo = (float)(tile_py + (w >> 1) * 4) + 0.5f, y_hi = y_lo + 3.f;
+    const float y_lo = (float)(tile_py + (w >> 1) * TileGeom<PX>::kBlockH) + 0.5f;
+    const float y_hi = y_lo + (float)(TileGeom<PX>::kBlockH - 1);
     if (x_lo <= mean.x + ex && x_hi >= mean.x - ex && y_lo <= mean.y + ey &&
         y_hi >= mean.y - ey)
       m |= 1u << w;

@@ -7,6 +7,7 @@
 namespace pxs {
 
 int g_fail_allocation_after = 0;
+int64_t g_device_allocations = 0;
 int64_t g_kernel_launches = 0;
 
 void check_cuda(cudaError_t err, const char* what) {

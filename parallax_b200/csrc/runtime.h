@@ -26,6 +26,9 @@ void check_cuda(cudaError_t err, const char* what);
 // Test hook: when positive, the n-th following device allocation fails as if
 // the device were out of memory (counted down per allocation).
 extern int g_fail_allocation_after;
+// Device allocations made by DeviceArray so far. A captured graph holds raw
+// buffer addresses, so it is stale once this has moved since the capture.
+extern int64_t g_device_allocations;
 
 // Grow-only device array; contents are not preserved across growth.
 template <typename T>
@@ -63,6 +66,7 @@ class DeviceArray {
                                          " bytes failed: " + cudaGetErrorString(err));
     }
     cap_ = count;
+    ++g_device_allocations;
     return ptr_;
   }
   void release() {

@@ -32,6 +32,8 @@ struct GraphState {
   int64_t pixels = -1, pair_capacity = -1, record_capacity = -1;
   int tiles = -1;
   int generation = -1;
+  int raster_generation = -1;
+  int64_t allocations = -1;
   bool timing = false;
   int64_t launches = 0;
   void reset() {
@@ -39,8 +41,8 @@ struct GraphState {
     if (graph != nullptr) cudaGraphDestroy(graph);
     exec = nullptr;
     graph = nullptr;
-    N = V = tiles = generation = -1;
-    pixels = pair_capacity = record_capacity = -1;
+    N = V = tiles = generation = raster_generation = -1;
+    pixels = pair_capacity = record_capacity = allocations = -1;
   }
 };
 
@@ -375,6 +377,73 @@ struct pxs_trainer {
                              cudaMemcpyDeviceToHost, stream));
   }
 
+  // Times the compositing kernels with 1, 2 and 4 pixels per thread on one
+  // batch of views and keeps the fastest forward and the fastest backward.
+  // The schedule, the parameters and the gradients are left as they were.
+  void autotune(int n_views, const int32_t* ids, int* forward_px, int* backward_px) {
+    std::vector<int> views;
+    for (int i = 0; i < n_views; ++i) {
+      const int id = ids != nullptr ? ids[i] : i % static_cast<int>(cameras.size());
+      if (id < 0 || id >= static_cast<int>(cameras.size()))
+        throw Error(PXS_ERR_INVALID, "view id out of range");
+      views.push_back(id);
+    }
+    const pxs::ViewBatch b = batch_for(views);
+    frame.prepare(b, N, S, stream);
+    frame.project(params.get(), stream);
+    frame.bin(true, stream);
+    float* d_dL = dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PXS_CUDA(cudaEventCreate(&e0));
+    PXS_CUDA(cudaEventCreate(&e1));
+    auto time_ms = [&](auto&& body) {
+      body();  // warm
+      PXS_CUDA(cudaEventRecord(e0, stream));
+      for (int r = 0; r < 3; ++r) body();
+      PXS_CUDA(cudaEventRecord(e1, stream));
+      PXS_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      PXS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
+    pxs::RasterConfig& rc = pxs::raster_config();
+    const int candidates[3] = {1, 2, 4};
+    float best = 0.f;
+    int best_fwd = rc.forward_px, best_bwd = rc.backward_px;
+    try {
+      for (int px : candidates) {
+        rc.forward_px = px;
+        const float ms = time_ms([&] { frame.forward(stream); });
+        if (px == candidates[0] || ms < best) {
+          best = ms;
+          best_fwd = px;
+        }
+      }
+      rc.forward_px = best_fwd;
+      frame.forward(stream);
+      frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
+      for (int px : candidates) {
+        rc.backward_px = px;
+        const float ms = time_ms([&] { frame.backward(d_dL, stream); });
+        if (px == candidates[0] || ms < best) {
+          best = ms;
+          best_bwd = px;
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rc.forward_px = best_fwd;
+    rc.backward_px = best_bwd;
+    ++rc.generation;
+    if (forward_px) *forward_px = best_fwd;
+    if (backward_px) *backward_px = best_bwd;
+  }
+
   // Batched step: every view of the batch in one pass of each kernel, one
   // Adam, optionally replayed from a captured CUDA graph.
   float step_batch(int n_views, const int32_t* ids, bool use_graph) {
@@ -398,7 +467,9 @@ struct pxs_trainer {
                            graph.pixels != b.total_pixels || graph.tiles != b.total_tiles ||
                            graph.pair_capacity != frame.pair_capacity ||
                            graph.record_capacity != frame.record_capacity ||
-                           graph.generation != generation;
+                           graph.generation != generation ||
+                           graph.raster_generation != pxs::raster_config().generation ||
+                           graph.allocations != pxs::g_device_allocations;
         if (stale) {
           graph.reset();
           const int64_t before = pxs::g_kernel_launches;
@@ -420,6 +491,8 @@ struct pxs_trainer {
           graph.pair_capacity = frame.pair_capacity;
           graph.record_capacity = frame.record_capacity;
           graph.generation = generation;
+          graph.raster_generation = pxs::raster_config().generation;
+          graph.allocations = pxs::g_device_allocations;
           graph.timing = timing;
           graph.launches = pxs::g_kernel_launches - before;
         }
@@ -608,6 +681,17 @@ int pxs_trainer_step_batch(pxs_trainer* t, int32_t n_views, const int32_t* view_
     if (n_views <= 0) throw Error(PXS_ERR_INVALID, "n_views must be positive");
     const float l = t->step_batch(n_views, view_ids, use_graph != 0);
     if (loss) *loss = l;
+  });
+}
+
+int pxs_trainer_autotune(pxs_trainer* t, int32_t n_views, const int32_t* view_ids,
+                         int32_t* forward_px, int32_t* backward_px) {
+  return guarded(t, [&] {
+    if (n_views <= 0) throw Error(PXS_ERR_INVALID, "n_views must be positive");
+    int f = 0, b = 0;
+    t->autotune(n_views, view_ids, &f, &b);
+    if (forward_px) *forward_px = f;
+    if (backward_px) *backward_px = b;
   });
 }
 

@@ -253,6 +253,35 @@ def test_backward_accumulates_rather_than_overwriting(ctx):
     assert max(errs.values()) <= 1e-5, errs
 
 
+@pytest.mark.parametrize("fwd_px,bwd_px", [(1, 1), (2, 2), (4, 4), (1, 4), (4, 1)])
+def test_pixels_per_thread_variants_agree(ctx, fwd_px, bwd_px):
+    """The compositing kernels at 1, 2 and 4 pixels per thread: the image and
+    the loss bit-identical, the gradients within 1e-4 normwise of the
+    reference (the adjoint only sums in another order)."""
+    lib = px.lib()
+    old_f, old_b = ct.c_int32(), ct.c_int32()
+    lib.pxs_get_raster_config(ct.byref(old_f), ct.byref(old_b))
+    d, view, opt, cloud = golden_case("raster_sh3.npz")
+    try:
+        assert lib.pxs_set_raster_config(fwd_px, bwd_px) == 0
+        rgb, T = px.render_splats(cloud, view.camera(), opt, ctx)
+        grads = px.SplatGradients.zeros(cloud)
+        loss = px.render_and_accumulate(cloud, view.camera(), opt, d["target"], 0.2, grads, ctx)
+        assert lib.pxs_set_raster_config(1, 1) == 0
+        rgb1, T1 = px.render_splats(cloud, view.camera(), opt, ctx)
+        grads1 = px.SplatGradients.zeros(cloud)
+        loss1 = px.render_and_accumulate(cloud, view.camera(), opt, d["target"], 0.2, grads1,
+                                         ctx)
+    finally:
+        lib.pxs_set_raster_config(old_f.value, old_b.value)
+    assert np.array_equal(rgb, rgb1) and np.array_equal(T, T1)
+    assert loss == loss1
+    assert np.array_equal(grads.visible_count, d["visible_count"])
+    errs = grad_errors(grads.params, d["grads"])
+    assert max(errs.values()) <= 1e-4, errs
+    assert lib.pxs_set_raster_config(3, 0) == px._abi.PXS_ERR_INVALID
+
+
 @pytest.mark.parametrize("name", ["raster_sh0.npz", "raster_sh3.npz"])
 def test_render_and_accumulate_matches_golden_reference(ctx, name):
     d, view, opt, cloud = golden_case(name)
