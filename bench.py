@@ -57,6 +57,9 @@ def parse_args():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--px", default="",
+                   help="pixels per thread 'F,B' for compositing and its adjoint "
+                        "(default: the autotuner picks)")
     return p.parse_args()
 
 
@@ -368,9 +371,14 @@ def run_ours(args):
 
     # the autotuner picks pixels per thread for compositing and its adjoint
     fpx, bpx = ct.c_int32(), ct.c_int32()
-    ids0 = (ct.c_int32 * V)(*ids_for(0))
-    trainer._check(lib.pxs_trainer_autotune(trainer.handle, V, ids0, ct.byref(fpx),
-                                            ct.byref(bpx)))
+    if args.px:
+        f_, b_ = (int(x) for x in args.px.split(","))
+        trainer._check(lib.pxs_set_raster_config(f_, b_))
+        lib.pxs_get_raster_config(ct.byref(fpx), ct.byref(bpx))
+    else:
+        ids0 = (ct.c_int32 * V)(*ids_for(0))
+        trainer._check(lib.pxs_trainer_autotune(trainer.handle, V, ids0, ct.byref(fpx),
+                                                ct.byref(bpx)))
 
     # warm-up: capture the graph, then once more with stage timing on
     for _ in range(max(args.warmup, 3)):

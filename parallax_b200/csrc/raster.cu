@@ -48,11 +48,11 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
   bool all_done = true;
 #pragma unroll
   for (int p = 0; p < PX; ++p) {
-    fy[p] = (float)(info.py0 + 4 * p) + 0.5f;
+    fy[p] = (float)(info.py0 + p) + 0.5f;
     T[p] = 1.f;
     acc0[p] = acc1[p] = acc2[p] = 0.f;
     last[p] = info.range.x;
-    done[p] = !(info.px < vd.cam.width && info.py0 + 4 * p < vd.cam.height);
+    done[p] = !(info.px < vd.cam.width && info.py0 + p < vd.cam.height);
     all_done = all_done && done[p];
   }
   unsigned long long evaluated = 0, contributing = 0;
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
   }
 #pragma unroll
   for (int p = 0; p < PX; ++p) {
-    const int py = info.py0 + 4 * p;
+    const int py = info.py0 + p;
     if (info.px < vd.cam.width && py < vd.cam.height) {
       const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
       rgb_out[pixel * 3 + 0] = acc0[p] + T[p] * vd.background[0];
@@ -126,6 +126,118 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
       rgb_out[pixel * 3 + 2] = acc2[p] + T[p] * vd.background[2];
       if (T_out != nullptr) T_out[pixel] = T[p];
       last_out[pixel] = last[p];
+    }
+  }
+  if (kCount) {
+    for (int o = 16; o > 0; o >>= 1) {
+      evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+      contributing += __shfl_xor_sync(0xffffffffu, contributing, o);
+    }
+    if (lane_id() == 0) {
+      atomicAdd(&counts[0], evaluated);
+      atomicAdd(&counts[1], contributing);
+    }
+  }
+}
+
+// The two-pixel form of k_forward: each thread composites two vertically
+// adjacent pixels of one column. Power, alpha and transmittance are the
+// scalar operations of k_forward (so the same entries are taken and T is
+// bit-identical); the colour sums of the two pixels are one paired fused
+// multiply-add per channel (fma.rn.f32x2), which differs from the separate
+// multiply and add by at most one rounding per entry. A pixel that does not
+// take an entry adds T * 0 * colour = 0.
+template <bool kCount>
+__global__ void __launch_bounds__(TileGeom<2>::kThreads)
+    k_forward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
+                 const float2* __restrict__ xy, const float4* __restrict__ conic_op,
+                 const float4* __restrict__ color, const ViewDesc* __restrict__ views,
+                 int n_views, float* __restrict__ rgb_out, float* __restrict__ T_out,
+                 int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts) {
+  constexpr int kThreads = TileGeom<2>::kThreads;
+  __shared__ float2 s_xy[kBatch];
+  __shared__ float4 s_co[kBatch];
+  __shared__ float4 s_col[kBatch];  // r, g, b, power floor
+  __shared__ uint32_t s_mask[kBatch];
+  const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
+  const int warp = threadIdx.x >> 5;
+  const ViewDesc& vd = views[info.view];
+  const float min_alpha = vd.min_alpha, cutoff = vd.transmittance_cutoff;
+  const float fx = (float)info.px + 0.5f;
+  const float2 fy = make_float2((float)info.py0 + 0.5f, (float)(info.py0 + 1) + 0.5f);
+  const bool col_in = info.px < vd.cam.width;
+  bool done0 = !(col_in && info.py0 < vd.cam.height);
+  bool done1 = !(col_in && info.py0 + 1 < vd.cam.height);
+  float2 T = make_float2(1.f, 1.f);
+  float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
+  int last0 = info.range.x, last1 = info.range.x;
+  unsigned long long evaluated = 0, contributing = 0;
+  for (int base = info.range.x; base < info.range.y; base += kBatch) {
+    if (__syncthreads_and(done0 && done1)) break;
+    const int n = min(kBatch, info.range.y - base);
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const uint32_t slot = pair_slots[base + i];
+      const float4 co = conic_op[slot];
+      const float2 mean = xy[slot];
+      float4 c = color[slot];
+      c.w = power_floor(co.w, min_alpha);
+      s_xy[i] = mean;
+      s_co[i] = co;
+      s_col[i] = c;
+      s_mask[i] = warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
+    }
+    __syncthreads();
+    if (!(done0 && done1)) {
+      for (int j = 0; j < n; ++j) {
+        if (kCount) evaluated += (done0 ? 0 : 1) + (done1 ? 0 : 1);
+        if (!((s_mask[j] >> warp) & 1u)) continue;  // cannot reach this warp's pixels
+        const float2 m = s_xy[j];
+        const float4 co = s_co[j];
+        const float floor = s_col[j].w;
+        const float dx = fx - m.x;
+        const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
+        const float2 power = splat_power2(co, dx, dy);
+        const bool in0 = !done0 && !(power.x > 0.f || power.x < floor);
+        const bool in1 = !done1 && !(power.y > 0.f || power.y < floor);
+        if (!(in0 || in1)) continue;
+        float a0 = in0 ? co.w * expf(power.x) : 0.f;
+        float a1 = in1 ? co.w * expf(power.y) : 0.f;
+        a0 = a0 < kMaxAlpha ? a0 : kMaxAlpha;
+        a1 = a1 < kMaxAlpha ? a1 : kMaxAlpha;
+        const bool c0 = in0 && !(a0 < min_alpha);
+        const bool c1 = in1 && !(a1 < min_alpha);
+        if (!(c0 || c1)) continue;
+        if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
+        const float4 c = s_col[j];
+        const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
+        acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
+        acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
+        acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
+        if (c0) {
+          T.x *= 1.f - a0;
+          last0 = base + j + 1;
+          if (T.x < cutoff) done0 = true;
+        }
+        if (c1) {
+          T.y *= 1.f - a1;
+          last1 = base + j + 1;
+          if (T.y < cutoff) done1 = true;
+        }
+        if (done0 && done1) break;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int py = info.py0 + p;
+    if (col_in && py < vd.cam.height) {
+      const float Tp = p ? T.y : T.x;
+      const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
+      rgb_out[pixel * 3 + 0] = (p ? acc0.y : acc0.x) + Tp * vd.background[0];
+      rgb_out[pixel * 3 + 1] = (p ? acc1.y : acc1.x) + Tp * vd.background[1];
+      rgb_out[pixel * 3 + 2] = (p ? acc2.y : acc2.x) + Tp * vd.background[2];
+      if (T_out != nullptr) T_out[pixel] = Tp;
+      last_out[pixel] = p ? last1 : last0;
     }
   }
   if (kCount) {
@@ -166,8 +278,8 @@ void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, co
                             total_tiles, rgb, T, last, stream, counts);
       break;
     default:
-      forward_px<kCount, 2>(ranges, pair_slots, xy, conic_op, color, views, n_views,
-                            total_tiles, rgb, T, last, stream, counts);
+      k_forward_x2<kCount><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
+          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts);
   }
 }
 

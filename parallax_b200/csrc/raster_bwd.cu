@@ -21,6 +21,9 @@ namespace pxs {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// At most this many contributing lanes: per-lane shared-memory atomics
+// instead of the warp-wide transpose reduction.
+constexpr int kDirectLanes = 2;
 
 // Sums v[0..9] over the warp. Returns, in ten of the even lanes, one complete
 // sum; *idx is the index of that value, or -1 in the other lanes.
@@ -90,7 +93,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
   int thread_hi = info.range.x;
 #pragma unroll
   for (int p = 0; p < PX; ++p) {
-    const int py = info.py0 + 4 * p;
+    const int py = info.py0 + p;
     fy[p] = (float)py + 0.5f;
     dLp0[p] = dLp1[p] = dLp2[p] = 0.f;
     final_T[p] = 1.f;
@@ -194,15 +197,235 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
           }
         }
       }
-      if (__any_sync(kFull, contrib)) {
-        const bool any_touched = __any_sync(kFull, touched);
-        int idx;
-        const float sum = warp_reduce10(v, lane, &idx);
+      const unsigned ballot = __ballot_sync(kFull, contrib);
+      if (ballot != 0u) {
         float* a = s_acc[j];
-        if (idx >= 0) atomicAdd(&a[idx], sum);
-        if (lane == 1) {
-          if (any_touched) atomicAdd(&a[10], 1.f);
-          a[11] = 1.f;
+        if (__popc(ballot) <= kDirectLanes) {
+          // few lanes: each adds its own sums, cheaper than the warp reduction
+          if (contrib) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) atomicAdd(&a[k], v[k]);
+            if (touched) a[10] = 1.f;
+            a[11] = 1.f;
+          }
+        } else {
+          const bool any_touched = __any_sync(kFull, touched);
+          int idx;
+          const float sum = warp_reduce10(v, lane, &idx);
+          if (idx >= 0) atomicAdd(&a[idx], sum);
+          if (lane == 1) {
+            if (any_touched) a[10] = 1.f;
+            a[11] = 1.f;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const float* a = s_acc[i];
+      if (a[11] != 0.f) {
+        float* dst = reinterpret_cast<float*>(&screen[s_slot[i]]);
+        red_add_v4(dst + 0, a[0], a[1], a[2], a[3]);
+        red_add_v4(dst + 4, a[4], a[5], a[6], a[7]);
+        red_add_v4(dst + 8, a[8], a[9], a[10], 0.f);
+      }
+    }
+  }
+}
+
+// The two-pixel form of k_backward: the gradient arithmetic of the two
+// vertically adjacent pixels of a thread runs as the halves of paired FP32
+// instructions (fma/add/mul .f32x2). The branch decisions are the forward's,
+// from the same scalar operations (splat_power2, alpha = opacity * exp). A
+// pixel that does not take an entry runs the paired arithmetic with alpha = 0
+// and a zero loss gradient, so its transmittance (multiplied by 1), its suffix
+// colour (an FMA with a zero weight) and its sums are unchanged.
+__global__ void __launch_bounds__(TileGeom<2>::kThreads)
+    k_backward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
+                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
+                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,
+                  int n_views, const float* __restrict__ T_final,
+                  const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
+                  ScreenGrad* __restrict__ screen) {
+  constexpr int kThreads = TileGeom<2>::kThreads;
+  __shared__ uint32_t s_slot[kBatch];
+  __shared__ float2 s_xy[kBatch];
+  __shared__ float4 s_co[kBatch];
+  __shared__ float4 s_col[kBatch];  // r, g, b, power floor
+  __shared__ uint32_t s_mask[kBatch];
+  __shared__ float s_acc[kBatch][12];
+  __shared__ int s_hi;
+  const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
+  const ViewDesc& vd = views[info.view];
+  const float min_alpha = vd.min_alpha;
+  const float fx = (float)info.px + 0.5f;
+  const float2 fy = make_float2((float)info.py0 + 0.5f, (float)(info.py0 + 1) + 0.5f);
+  float2 dLp0 = make_float2(0.f, 0.f), dLp1 = dLp0, dLp2 = dLp0;
+  float2 T = make_float2(1.f, 1.f);
+  int last0 = info.range.x, last1 = info.range.x;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int py = info.py0 + p;
+    if (info.px < vd.cam.width && py < vd.cam.height) {
+      const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
+      const float d0 = dL_drgb[pixel * 3 + 0], d1 = dL_drgb[pixel * 3 + 1];
+      const float d2 = dL_drgb[pixel * 3 + 2], tf = T_final[pixel];
+      const int l = last_in[pixel];
+      if (p == 0) {
+        dLp0.x = d0; dLp1.x = d1; dLp2.x = d2; T.x = tf; last0 = l;
+      } else {
+        dLp0.y = d0; dLp1.y = d1; dLp2.y = d2; T.y = tf; last1 = l;
+      }
+    }
+  }
+  // final T times the background's share of the loss gradient
+  const float2 bg_term = __fmul2_rn(
+      T, __ffma2_rn(make_float2(vd.background[2], vd.background[2]), dLp2,
+                    __ffma2_rn(make_float2(vd.background[1], vd.background[1]), dLp1,
+                               __fmul2_rn(make_float2(vd.background[0], vd.background[0]),
+                                          dLp0))));
+  float2 suffix0 = make_float2(0.f, 0.f), suffix1 = suffix0, suffix2 = suffix0;
+  float2 last_alpha = suffix0, lc0 = suffix0, lc1 = suffix0, lc2 = suffix0;
+  const int lane = lane_id(), warp = warp_id();
+  const int warp_hi = __reduce_max_sync(kFull, max(last0, last1));
+  if (threadIdx.x == 0) s_hi = info.range.x;
+  __syncthreads();
+  if (lane == 0 && warp_hi > info.range.x) atomicMax(&s_hi, warp_hi);
+  __syncthreads();
+  const int hi = s_hi;
+  const float2 one = make_float2(1.f, 1.f);
+
+  for (int batch_end = hi; batch_end > info.range.x; batch_end -= kBatch) {
+    const int batch_start = max(info.range.x, batch_end - kBatch);
+    const int n = batch_end - batch_start;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const uint32_t slot = pair_slots[batch_start + i];
+      const float4 co = conic_op[slot];
+      const float2 mean = xy[slot];
+      float4 c = color[slot];
+      c.w = power_floor(co.w, min_alpha);
+      s_slot[i] = slot;
+      s_xy[i] = mean;
+      s_co[i] = co;
+      s_col[i] = c;
+      s_mask[i] = warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) s_acc[i][k] = 0.f;
+    }
+    __syncthreads();
+    const int j_top = min(n, warp_hi - batch_start) - 1;  // warp-uniform
+    for (int j = j_top; j >= 0; --j) {
+      if (!((s_mask[j] >> warp) & 1u)) continue;  // cannot reach this warp's pixels
+      const int e = batch_start + j;
+      const float2 m = s_xy[j];
+      const float4 co = s_co[j];
+      const float4 c = s_col[j];
+      const float dx = fx - m.x;
+      const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
+      const float2 power = splat_power2(co, dx, dy);
+      const bool in0 = e < last0 && !(power.x > 0.f) && !(power.x < c.w);
+      const bool in1 = e < last1 && !(power.y > 0.f) && !(power.y < c.w);
+      bool contrib = false, touched = false;
+      float v[10];
+#pragma unroll
+      for (int k = 0; k < 10; ++k) v[k] = 0.f;
+      if (in0 || in1) {
+        const float g0 = in0 ? expf(power.x) : 0.f;
+        const float g1 = in1 ? expf(power.y) : 0.f;
+        const float r0 = __fmul_rn(co.w, g0), r1 = __fmul_rn(co.w, g1);
+        const float a0 = r0 < kMaxAlpha ? r0 : kMaxAlpha;
+        const float a1 = r1 < kMaxAlpha ? r1 : kMaxAlpha;
+        const bool c0 = in0 && !(a0 < min_alpha);
+        const bool c1 = in1 && !(a1 < min_alpha);
+        if (c0 || c1) {
+          contrib = true;
+          const float2 alpha = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
+          const float2 inv = make_float2(c0 ? __fdividef(1.f, 1.f - alpha.x) : 1.f,
+                                         c1 ? __fdividef(1.f, 1.f - alpha.y) : 1.f);
+          T = __fmul2_rn(T, inv);
+          const float2 weight = __fmul2_rn(alpha, T);
+          const float2 w6 = __fmul2_rn(weight, dLp0);
+          const float2 w7 = __fmul2_rn(weight, dLp1);
+          const float2 w8 = __fmul2_rn(weight, dLp2);
+          v[6] = w6.x + w6.y;
+          v[7] = w7.x + w7.y;
+          v[8] = w8.x + w8.y;
+          // suffix = la * lc + (1 - la) * suffix, only where this entry counts
+          const float2 la = make_float2(c0 ? last_alpha.x : 0.f, c1 ? last_alpha.y : 0.f);
+          const float2 keep = __fadd2_rn(one, make_float2(-la.x, -la.y));
+          suffix0 = __ffma2_rn(la, lc0, __fmul2_rn(keep, suffix0));
+          suffix1 = __ffma2_rn(la, lc1, __fmul2_rn(keep, suffix1));
+          suffix2 = __ffma2_rn(la, lc2, __fmul2_rn(keep, suffix2));
+          if (c0) {
+            lc0.x = c.x; lc1.x = c.y; lc2.x = c.z; last_alpha.x = alpha.x;
+          }
+          if (c1) {
+            lc0.y = c.x; lc1.y = c.y; lc2.y = c.z; last_alpha.y = alpha.y;
+          }
+          float2 dL_dalpha = __fmul2_rn(
+              __ffma2_rn(__fadd2_rn(make_float2(c.z, c.z), make_float2(-suffix2.x, -suffix2.y)),
+                         dLp2,
+                         __ffma2_rn(__fadd2_rn(make_float2(c.y, c.y),
+                                               make_float2(-suffix1.x, -suffix1.y)),
+                                    dLp1,
+                                    __fmul2_rn(__fadd2_rn(make_float2(c.x, c.x),
+                                                          make_float2(-suffix0.x, -suffix0.y)),
+                                               dLp0))),
+              T);
+          dL_dalpha = __ffma2_rn(make_float2(-inv.x, -inv.y), bg_term, dL_dalpha);
+          // the 0.99 cap flattens the gradient
+          const bool t0 = c0 && r0 < kMaxAlpha, t1 = c1 && r1 < kMaxAlpha;
+          if (t0 || t1) {
+            touched = true;
+            const float2 z = make_float2(t0 ? dL_dalpha.x : 0.f, t1 ? dL_dalpha.y : 0.f);
+            const float2 gw = make_float2(g0, g1);
+            const float2 q = __fmul2_rn(gw, z);          // dL/dopacity per pixel
+            const float2 dLw = __fmul2_rn(make_float2(co.w, co.w), z);
+            const float2 gx = __fmul2_rn(gw, make_float2(dx, dx));
+            const float2 gy = __fmul2_rn(gw, dy);
+            // d(mean) = -d(delta): v0 = -dm0, v1 = -dm1
+            const float2 dm0 = __fmul2_rn(
+                dLw, __ffma2_rn(gy, make_float2(-co.y, -co.y),
+                                __fmul2_rn(gx, make_float2(-co.x, -co.x))));
+            const float2 dm1 = __fmul2_rn(
+                dLw, __ffma2_rn(gx, make_float2(-co.y, -co.y),
+                                __fmul2_rn(gy, make_float2(-co.z, -co.z))));
+            const float2 sq = __ffma2_rn(dm1, dm1, __fmul2_rn(dm0, dm0));
+            const float2 wx = __fmul2_rn(dLw, gx);
+            const float2 wy = __fmul2_rn(dLw, gy);
+            const float2 d2 = __fmul2_rn(wx, make_float2(-0.5f * dx, -0.5f * dx));
+            const float2 d3 = __fmul2_rn(wx, make_float2(-dy.x, -dy.y));
+            const float2 d4 = __fmul2_rn(wy, __fmul2_rn(make_float2(-0.5f, -0.5f), dy));
+            v[0] = -(dm0.x + dm0.y);
+            v[1] = -(dm1.x + dm1.y);
+            v[2] = d2.x + d2.y;
+            v[3] = d3.x + d3.y;
+            v[4] = d4.x + d4.y;
+            v[5] = q.x + q.y;
+            v[9] = sqrtf(sq.x) + sqrtf(sq.y);
+          }
+        }
+      }
+      const unsigned ballot = __ballot_sync(kFull, contrib);
+      if (ballot != 0u) {
+        float* a = s_acc[j];
+        if (__popc(ballot) <= kDirectLanes) {
+          if (contrib) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) atomicAdd(&a[k], v[k]);
+            if (touched) a[10] = 1.f;
+            a[11] = 1.f;
+          }
+        } else {
+          const bool any_touched = __any_sync(kFull, touched);
+          int idx;
+          const float sum = warp_reduce10(v, lane, &idx);
+          if (idx >= 0) atomicAdd(&a[idx], sum);
+          if (lane == 1) {
+            if (any_touched) a[10] = 1.f;
+            a[11] = 1.f;
+          }
         }
       }
     }
@@ -248,8 +471,9 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
                      T_final, last, dL_drgb, screen, stream);
       break;
     default:
-      backward_px<2>(ranges, pair_slots, xy, conic_op, color, views, n_views, total_tiles,
-                     T_final, last, dL_drgb, screen, stream);
+      k_backward_x2<<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
+          ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
+          screen);
   }
 }
 

@@ -12,8 +12,8 @@ namespace pxs {
 constexpr int kBatch = 256;
 
 // Pixels per thread. A warp covers an 8-wide block of 4*PX rows: lane l owns
-// column l%8 and rows l/8 + 4p (p < PX); warp w covers columns 8*(w%2) .. +8
-// and rows 4*PX*(w/2) .. +4*PX of the 16x16 tile. PX = 1 gives 8 warps of 8x4,
+// column l%8 and the PX adjacent rows PX*(l/8) + p (p < PX); warp w covers
+// columns 8*(w%2) .. +8 and rows 4*PX*(w/2) .. +4*PX of the 16x16 tile. PX = 1 gives 8 warps of 8x4,
 // PX = 2 4 warps of 8x8, PX = 4 2 warps of 8x16. More pixels per thread share
 // each staged entry and each warp-level reduction among more pixels.
 template <int PX>
@@ -27,7 +27,7 @@ template <int PX>
 struct TileInfo {
   int view;
   int px;      // this thread's column
-  int py0;     // its first row; pixel p is at row py0 + 4p
+  int py0;     // its first row; pixel p is at row py0 + p
   int tile_px, tile_py;
   int2 range;
 };
@@ -45,7 +45,7 @@ __device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ v
   info.tile_px = tx * kTile;
   info.tile_py = ty * kTile;
   info.px = info.tile_px + (w & 1) * 8 + (lane & 7);
-  info.py0 = info.tile_py + (w >> 1) * TileGeom<PX>::kBlockH + (lane >> 3);
+  info.py0 = info.tile_py + (w >> 1) * TileGeom<PX>::kBlockH + PX * (lane >> 3);
   info.range = ranges[tile];
   return info;
 }
@@ -88,6 +88,20 @@ __device__ __forceinline__ float splat_power(const float4& co, float dx, float d
   const float t2 = __fmul_rn(__fmul_rn(co.z, dy), dy);
   const float t3 = __fmul_rn(__fmul_rn(co.y, dx), dy);
   return __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2)), t3);
+}
+
+// splat_power for the two pixels (dx, dy.x) and (dx, dy.y) of one column:
+// the same scalar operations, with the products that only involve dx shared.
+// (Paired f32x2 instructions are not used here: the code generator may fuse a
+// paired multiply and add into one rounding, and these values decide which
+// entries a pixel takes, so they must round exactly like the reference.)
+__device__ __forceinline__ float2 splat_power2(const float4& co, float dx, float2 dy) {
+  const float t1 = __fmul_rn(__fmul_rn(co.x, dx), dx);
+  const float bdx = __fmul_rn(co.y, dx);
+  const float t2x = __fmul_rn(__fmul_rn(co.z, dy.x), dy.x);
+  const float t2y = __fmul_rn(__fmul_rn(co.z, dy.y), dy.y);
+  return make_float2(__fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2x)), __fmul_rn(bdx, dy.x)),
+                     __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2y)), __fmul_rn(bdx, dy.y)));
 }
 
 // A power below which opacity * exp(power) is certainly under min_alpha, so

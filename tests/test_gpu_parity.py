@@ -255,9 +255,10 @@ def test_backward_accumulates_rather_than_overwriting(ctx):
 
 @pytest.mark.parametrize("fwd_px,bwd_px", [(1, 1), (2, 2), (4, 4), (1, 4), (4, 1)])
 def test_pixels_per_thread_variants_agree(ctx, fwd_px, bwd_px):
-    """The compositing kernels at 1, 2 and 4 pixels per thread: the image and
-    the loss bit-identical, the gradients within 1e-4 normwise of the
-    reference (the adjoint only sums in another order)."""
+    """The compositing kernels at 1, 2 and 4 pixels per thread: the same
+    entries taken (transmittance bit-identical), colours within 1e-6 (the
+    two-pixel form sums colour with fused multiply-adds), the gradients within
+    1e-4 normwise of the reference (the adjoint sums in another order)."""
     lib = px.lib()
     old_f, old_b = ct.c_int32(), ct.c_int32()
     lib.pxs_get_raster_config(ct.byref(old_f), ct.byref(old_b))
@@ -274,8 +275,9 @@ def test_pixels_per_thread_variants_agree(ctx, fwd_px, bwd_px):
                                          ctx)
     finally:
         lib.pxs_set_raster_config(old_f.value, old_b.value)
-    assert np.array_equal(rgb, rgb1) and np.array_equal(T, T1)
-    assert loss == loss1
+    assert np.array_equal(T, T1)
+    assert np.abs(rgb - rgb1).max() <= 1e-6 * max(1.0, np.abs(rgb1).max())
+    assert abs(loss - loss1) <= 1e-5 * abs(loss1)
     assert np.array_equal(grads.visible_count, d["visible_count"])
     errs = grad_errors(grads.params, d["grads"])
     assert max(errs.values()) <= 1e-4, errs
