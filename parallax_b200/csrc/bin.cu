@@ -8,14 +8,16 @@
 //   1. each visible splat (in depth order) emits one record per tile row it
 //      covers -- (global row id, slot), about one seventh as many as pairs;
 //   2. one stable radix pass groups the records by row, keeping depth order;
-//   3. each row is cut into chunks of 2048 records; one CTA per chunk counts,
+//   3. each row is cut into chunks of 1024 records; one CTA per chunk counts,
 //      per column, the records covering it; a per-row pass turns those into
 //      each chunk's base within every tile of the row and the tiles' lengths;
 //      an exclusive scan over the tiles gives the tile ranges;
 //   4. one CTA per chunk walks its records again, 32 at a time per warp: each
 //      lane sets its bit in a per-column bitmap for every column its splat
-//      covers, and the pair's place in the tile's list is the column's running
-//      base plus the number of earlier lanes in the bitmap.
+//      covers, and the pair's place among the chunk's pairs of that column is
+//      the column's running base plus the number of earlier lanes in the
+//      bitmap; the chunk's pairs are grouped by column in shared memory and
+//      copied out to the lists with consecutive stores.
 // The result -- ranges and slot lists -- is exactly the reference's, with
 // equal depths in gaussian order (the depth sort is stable over slots).
 #include "common.cuh"
@@ -106,7 +108,8 @@ __global__ void __launch_bounds__(256)
 // Rows are cut into chunks of at most kChunk records so the work balances
 // whatever the rows' lengths. chunks[c] = (row, begin, end); n_chunks[0] is
 // the count. One CTA builds the table with a block-wide scan over the rows.
-constexpr int kChunk = 2048;
+constexpr int kChunk = 1024;
+constexpr int kStage = 16384;  // pairs a chunk can stage in shared memory
 constexpr int kPerLane = kChunk / (kWarps * 32);  // records per lane per chunk
 
 __global__ void __launch_bounds__(1024)
@@ -256,9 +259,40 @@ __global__ void k_ranges_from_offsets(const int32_t* __restrict__ counts,
   }
 }
 
+// Block-wide exclusive scan of v (one value per thread); returns the prefix
+// and writes the total to *total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
+  const int lane = lane_id(), w = warp_id();
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int n = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += n;
+  }
+  if (lane == 31) s_warp[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int y = lane < kWarps ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < kWarps; o <<= 1) {
+      const int n = __shfl_up_sync(kFull, y, o);
+      if (lane >= o) y += n;
+    }
+    if (lane < kWarps) s_warp[lane] = y;
+  }
+  __syncthreads();
+  const int before = (w > 0 ? s_warp[w - 1] : 0) + x - v;
+  *total = s_warp[kWarps - 1];
+  __syncthreads();
+  return before;
+}
+
 // Writes each chunk's records into its row's tile lists, in record (depth)
 // order: 32 records at a time per warp, a per-column bitmap giving each pair
-// its place among the lanes.
+// its place among the lanes. The chunk's pairs are staged in shared memory
+// grouped by column, then copied out column by column, so each tile's run of
+// the chunk is written with consecutive stores; a chunk with more pairs than
+// the stage holds stores them straight into the lists instead.
 __global__ void __launch_bounds__(kWarps * 32)
     k_chunk_expand(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
                    const uint32_t* __restrict__ rec_slots, const uint2* __restrict__ rect,
@@ -266,7 +300,10 @@ __global__ void __launch_bounds__(kWarps * 32)
                    const int32_t* __restrict__ chunk_base,
                    const int64_t* __restrict__ tile_offsets, int64_t capacity,
                    uint32_t* __restrict__ tile_slots) {
-  extern __shared__ int32_t s_mem[];  // counts/base [kWarps][max_tiles_x], bitmap same shape
+  // [kWarps][max_tiles_x] counts then bases, the same shape of bitmaps,
+  // per column: stage start, pair count and list position; then the stage
+  extern __shared__ __align__(16) int32_t s_mem[];
+  __shared__ int s_warp[kWarps];
   if ((int)blockIdx.x >= n_chunks[0]) return;
   const int4 ch = chunks[blockIdx.x];
   const ViewDesc& vd = views[view_of_row(views, n_views, ch.x)];
@@ -274,6 +311,11 @@ __global__ void __launch_bounds__(kWarps * 32)
   const int w = warp_id(), lane = lane_id();
   int32_t* s_cnt = s_mem;
   uint32_t* bitmap_all = reinterpret_cast<uint32_t*>(s_mem + kWarps * max_tiles_x);
+  int32_t* col_start = s_mem + 2 * kWarps * max_tiles_x;
+  int32_t* col_count = col_start + max_tiles_x;
+  // at byte 72 * max_tiles_x of the 16-byte aligned block: 8-byte aligned
+  int64_t* col_dst = reinterpret_cast<int64_t*>(col_count + max_tiles_x);
+  uint32_t* stage = reinterpret_cast<uint32_t*>(col_dst + max_tiles_x);
   for (int i = threadIdx.x; i < kWarps * tiles_x; i += blockDim.x) {
     s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
     bitmap_all[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0u;
@@ -282,16 +324,34 @@ __global__ void __launch_bounds__(kWarps * 32)
   uint32_t slot[kPerLane], xr[kPerLane];
   chunk_column_counts(ch, rec_slots, rect, max_tiles_x, s_cnt, slot, xr);
   __syncthreads();
-  // per column: exclusive prefix over warps, plus the chunk's base and the tile's offset
+  // per-column totals, then their exclusive scan: each column's stage start
+  const int per = (tiles_x + blockDim.x - 1) / blockDim.x;
+  const int c_begin = min(tiles_x, (int)threadIdx.x * per);
+  const int c_end = min(tiles_x, c_begin + per);
+  int mine = 0;
+  for (int c = c_begin; c < c_end; ++c) {
+    int t = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) t += s_cnt[k * max_tiles_x + c];
+    col_count[c] = t;
+    mine += t;
+  }
+  int total = 0;
+  int run_start = block_exclusive_scan(mine, s_warp, &total);
+  const bool staged = total <= kStage;  // block-uniform
   const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)(ch.x - vd.row_offset) * tiles_x;
-  for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
-    int run = (int)tile_offsets[tile0 + c] + chunk_base[(int64_t)blockIdx.x * max_tiles_x + c];
+  for (int c = c_begin; c < c_end; ++c) {
+    col_start[c] = run_start;
+    col_dst[c] = tile_offsets[tile0 + c] + chunk_base[(int64_t)blockIdx.x * max_tiles_x + c];
+    // per warp, where its pairs of this column begin among the chunk's pairs
+    int run = run_start;
 #pragma unroll
     for (int k = 0; k < kWarps; ++k) {
       const int t = s_cnt[k * max_tiles_x + c];
       s_cnt[k * max_tiles_x + c] = run;
       run += t;
     }
+    run_start += col_count[c];
   }
   __syncthreads();
   int32_t* base = s_cnt + w * max_tiles_x;
@@ -303,8 +363,13 @@ __global__ void __launch_bounds__(kWarps * 32)
     for (int c = x0; c <= x1; ++c) atomicOr(&bitmap[c], 1u << lane);
     __syncwarp();
     for (int c = x0; c <= x1; ++c) {
-      const int64_t pos = (int64_t)base[c] + __popc(bitmap[c] & lt);
-      if (pos < capacity) tile_slots[pos] = slot[k];
+      const int pos = base[c] + __popc(bitmap[c] & lt);  // among the chunk's pairs
+      if (staged) {
+        stage[pos] = slot[k];
+      } else {
+        const int64_t dst = col_dst[c] + (pos - col_start[c]);
+        if (dst < capacity) tile_slots[dst] = slot[k];
+      }
     }
     __syncwarp();
     const int lo = __reduce_min_sync(kFull, x1 >= x0 ? x0 : (1 << 30));
@@ -317,6 +382,15 @@ __global__ void __launch_bounds__(kWarps * 32)
       }
     }
     __syncwarp();
+  }
+  if (!staged) return;
+  __syncthreads();
+  // copy out: one warp per column, consecutive entries per lane
+  for (int c = w; c < tiles_x; c += kWarps) {
+    const int n = col_count[c], src = col_start[c];
+    const int64_t dst = col_dst[c];  // >= 0: offsets and bases are counts
+    for (int i = lane; i < n; i += 32)
+      if (dst + i < capacity) tile_slots[dst + i] = stage[src + i];
   }
 }
 
@@ -343,7 +417,10 @@ void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const
 }
 
 size_t chunk_counts_smem(int max_tiles_x) { return sizeof(int32_t) * kWarps * max_tiles_x; }
-size_t chunk_expand_smem(int max_tiles_x) { return 2 * sizeof(int32_t) * kWarps * max_tiles_x; }
+size_t chunk_expand_smem(int max_tiles_x) {
+  return sizeof(int32_t) * ((2 * kWarps + 2) * (size_t)max_tiles_x + kStage) +
+         sizeof(int64_t) * (size_t)max_tiles_x;
+}
 
 void configure_bin_kernels() {
   cudaFuncSetAttribute(k_chunk_counts, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -54,19 +54,25 @@ __global__ void __launch_bounds__(kThreads)
   const int tid = threadIdx.x;
 
   // stage both images over the input region, zero outside
-  for (int i = tid; i < IH * IW * 3; i += kThreads) {
-    const int c = i % 3;
-    const int q = i / 3;
+  for (int q = tid; q < IH * IW; q += kThreads) {
     const int lx = q % IW, ly = q / IW;
     const int X = ox - 10 + lx, Y = oy - 10 + ly;
-    float a = 0.f, b = 0.f;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
     if (X >= 0 && X < W && Y >= 0 && Y < H) {
-      const int64_t o = ((int64_t)Y * W + X) * 3 + c;
-      a = rimg[o];
-      b = timg[o];
+      const int64_t o = ((int64_t)Y * W + X) * 3;
+      a0 = rimg[o];
+      a1 = rimg[o + 1];
+      a2 = rimg[o + 2];
+      b0 = timg[o];
+      b1 = timg[o + 1];
+      b2 = timg[o + 2];
     }
-    sm.in_r[c][ly][lx] = a;
-    sm.in_t[c][ly][lx] = b;
+    sm.in_r[0][ly][lx] = a0;
+    sm.in_r[1][ly][lx] = a1;
+    sm.in_r[2][ly][lx] = a2;
+    sm.in_t[0][ly][lx] = b0;
+    sm.in_t[1][ly][lx] = b1;
+    sm.in_t[2][ly][lx] = b2;
   }
   __syncthreads();
 
@@ -85,23 +91,26 @@ __global__ void __launch_bounds__(kThreads)
       constexpr int HS = 6;
       for (int item = tid; item < IH * (SW / HS); item += kThreads) {
         const int r = item / (SW / HS), col0 = (item % (SW / HS)) * HS;
-        float xs[HS + 10], ys[HS + 10];
+        float xs[HS + 10], ys[HS + 10], xx[HS + 10], yy[HS + 10], xy[HS + 10];
 #pragma unroll
         for (int k = 0; k < HS + 10; ++k) {
           xs[k] = sm.in_r[c][r][col0 + k];
           ys[k] = sm.in_t[c][r][col0 + k];
+          xx[k] = xs[k] * xs[k];
+          yy[k] = ys[k] * ys[k];
+          xy[k] = xs[k] * ys[k];
         }
 #pragma unroll
         for (int o = 0; o < HS; ++o) {
           float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f;
 #pragma unroll
           for (int k = 0; k < 11; ++k) {
-            const float x = xs[o + k], y = ys[o + k], kk = lp.kernel[k];
-            s0 += kk * x;
-            s1 += kk * y;
-            s2 += kk * (x * x);
-            s3 += kk * (y * y);
-            s4 += kk * (x * y);
+            const float kk = lp.kernel[k];
+            s0 += kk * xs[o + k];
+            s1 += kk * ys[o + k];
+            s2 += kk * xx[o + k];
+            s3 += kk * yy[o + k];
+            s4 += kk * xy[o + k];
           }
           sm.hb[0][r][col0 + o] = s0;
           sm.hb[1][r][col0 + o] = s1;
@@ -145,11 +154,13 @@ __global__ void __launch_bounds__(kThreads)
             const float b = 2.f * cov + c2;
             const float cc = mu_x * mu_x + mu_y * mu_y + c1;
             const float d = var_x + var_y + c2;
-            if (col >= 5 && col < 5 + TW && r >= 5 && r < 5 + TH)
-              ssim_sum += (double)((a * b) / (cc * d));
-            t_mu = scale * (2.f * mu_y * b / (cc * d) - 2.f * mu_x * a * b / (cc * cc * d));
-            t_var = scale * (-(a * b) / (cc * d * d));
-            t_cov = scale * (2.f * a / (cc * d));
+            const float rc = 1.f / cc, rd = 1.f / d;
+            const float r_ccd = rc * rd;  // 1 / (cc d)
+            const float ssim = (a * b) * r_ccd;
+            if (col >= 5 && col < 5 + TW && r >= 5 && r < 5 + TH) ssim_sum += (double)ssim;
+            t_mu = scale * (2.f * b * r_ccd) * (mu_y - mu_x * a * rc);
+            t_var = -scale * ssim * rd;
+            t_cov = scale * (2.f * a * r_ccd);
           } else {
             mu_x = 0.f;
             mu_y = 0.f;
