@@ -296,7 +296,7 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import parallax_b200 as px
     from parallax_b200.scenes import WORKLOADS, workload_scene
 
@@ -335,8 +335,18 @@ def run_ours(args):
         base = (step * V + rank * 7) % pool
         return [(base + i) % pool for i in range(V)]
 
-    def batch_step(step, graph=True):
-        return trainer.step_batch(V, ids_for(step), graph=graph)
+    if world > 1:
+        # data parallel over views: each rank renders its own V views, the
+        # gradient buffers are summed over the ranks, every rank takes the
+        # same Adam step
+        from parallax_b200.data_parallel import DataParallelStep
+        dp_step = DataParallelStep(trainer, device="cuda")
+
+        def batch_step(step, graph=True):
+            return dp_step(ids_for(step))
+    else:
+        def batch_step(step, graph=True):
+            return trainer.step_batch(V, ids_for(step), graph=graph)
 
     def barrier():
         if world > 1:
@@ -408,7 +418,7 @@ def run_ours(args):
 
     result = {}
     ms_plain = None
-    if not args.no_plain:
+    if not args.no_plain and world == 1:
         def plain_step(_):
             step_counter[0] += 1
             trainer.step_views(V, ids_for(step_counter[0]))
@@ -423,7 +433,7 @@ def run_ours(args):
             id_arr = (ct.c_int32 * V)(*ids)
             ptrs = (ct.c_void_p * V)(*[pinned[i][1].ctypes.data for i in ids])
             trainer._check(lib.pxs_trainer_set_images(trainer.handle, V, id_arr, ptrs))
-            trainer.step_batch(V, ids, graph=True)  # reads the loss back to the host
+            batch_step(step_counter[0])  # reads the loss back to the host
         e2e_step(0)
         ms_e2e = timed(e2e_step, args.steps)
         h2d = sum(views[i].width * views[i].height * 3 * 4 for i in ids_for(0))

@@ -318,6 +318,25 @@ int pxs_trainer_train(pxs_trainer* trainer, pxs_progress_fn callback, void* user
 int pxs_trainer_step_batch(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                            int32_t graph, float* loss);
 
+/* The data-parallel split of pxs_trainer_step_batch, for one trainer per GPU
+ * over a shared cloud. pxs_trainer_accumulate renders and differentiates this
+ * rank's `n_views` views (a graph replay when `graph` is nonzero) and leaves
+ * the summed gradients in the trainer's device buffers with no optimiser
+ * step; `loss` gets the mean loss of these views. The caller then sums the
+ * buffers of pxs_trainer_gradients over the ranks (an all-reduce in place,
+ * on or after the trainer's stream) and calls pxs_trainer_apply with the mean
+ * loss over all ranks' views, which takes the Adam step and the schedule's
+ * densify / opacity reset. Ranks that apply identical sums stay identical.
+ * pxs_trainer_gradients returns device pointers: the gradient array
+ * (values x count floats in the parameter layout), the screen gradient
+ * (count floats) and the visible count (count int32), valid until the cloud
+ * is resized (densify). */
+int pxs_trainer_accumulate(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
+                           int32_t graph, float* loss);
+int pxs_trainer_apply(pxs_trainer* trainer, float loss);
+int pxs_trainer_gradients(pxs_trainer* trainer, float** params, float** screen_gradient,
+                          int32_t** visible_count, int32_t* count, int32_t* values);
+
 /* Plain form of the same multi-view step: per-view kernel sequences with
  * host-synchronised sizes and no graph. Same arithmetic, same result. */
 int pxs_trainer_step_views(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,

@@ -72,6 +72,9 @@ def _declare(lib: ct.CDLL) -> None:
         "pxs_set_raster_config": (ct.c_int, [_i32, _i32]),
         "pxs_get_raster_config": (ct.c_int, [_vp, _vp]),
         "pxs_trainer_autotune": (ct.c_int, [_vp, _i32, _vp, _vp, _vp]),
+        "pxs_trainer_accumulate": (ct.c_int, [_vp, _i32, _vp, _i32, _vp]),
+        "pxs_trainer_apply": (ct.c_int, [_vp, _f32]),
+        "pxs_trainer_gradients": (ct.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
         "pxs_synthetic_cloud": (ct.c_int, [ct.c_uint64, _i32, _i32, _f32, _vp]),
         "pxs_synthetic_cameras": (ct.c_int, [ct.c_uint64, _i32, _i32, ct.c_double, _i32, _i32,
                                              ct.c_double, _vp]),

@@ -77,7 +77,9 @@ struct pxs_trainer {
   pxs::DensifyWork dwork;
   DeviceArray<pxs::StepScalars> scalars;
   DeviceArray<float> dL, loss_acc;
-  pxs::GraphState graph;
+  pxs::GraphState graph;      // the batched step
+  pxs::GraphState graph_acc;  // its data-parallel accumulate half
+  bool pending_apply = false;
   int generation = 0;  // bumped whenever a state buffer is reallocated
   float* host_loss = nullptr;     // pinned
   int32_t* host_overflow = nullptr;
@@ -95,6 +97,7 @@ struct pxs_trainer {
 
   ~pxs_trainer() {
     graph.reset();
+    graph_acc.reset();
     for (cudaEvent_t& e : events)
       if (e) cudaEventDestroy(e);
     if (host_loss) cudaFreeHost(host_loss);
@@ -351,8 +354,9 @@ struct pxs_trainer {
     ++timed_steps;
   }
 
-  // Enqueues the batched step body (everything after the view upload).
-  void enqueue_batch_body() {
+  // Enqueues the batched step body (everything after the view upload); the
+  // optimiser step is left out for the data-parallel split (accumulate).
+  void enqueue_batch_body(bool with_adam) {
     mark(0);
     frame.project(params.get(), stream);
     mark(1);
@@ -367,14 +371,93 @@ struct pxs_trainer {
     frame.param_grads(params.get(), grads.get(), screen_gradient.get(), visible_count.get(),
                       stream);
     mark(6);
-    pxs::launch_adam_checked(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(),
-                             screen_gradient.get(), visible_count.get(), acc_gradient.get(),
-                             acc_views.get(), frame.overflow.get(), stream);
+    if (with_adam)
+      pxs::launch_adam_checked(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(),
+                               screen_gradient.get(), visible_count.get(), acc_gradient.get(),
+                               acc_views.get(), frame.overflow.get(), stream);
     mark(7);
     PXS_CUDA(cudaMemcpyAsync(host_loss, frame.loss_total.get(), sizeof(float),
                              cudaMemcpyDeviceToHost, stream));
     PXS_CUDA(cudaMemcpyAsync(host_overflow, frame.overflow.get(), sizeof(int32_t),
                              cudaMemcpyDeviceToHost, stream));
+  }
+
+  // Runs the batched body for `views`, replayed from `g` when use_graph, and
+  // redoes it with larger pair buffers while the pairs overflow. The
+  // optimiser, when included, skips a step whose pairs overflowed.
+  void run_batch(const std::vector<int>& views, bool use_graph, bool with_adam,
+                 pxs::GraphState& g) {
+    const pxs::ViewBatch b = batch_for(views);
+    frame.prepare(b, N, S, stream);  // also uploads the view descriptors
+    dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
+    if (frame.pair_capacity == 0 || frame.record_capacity == 0) {
+      // learn the pair count once, then run unsynchronised with headroom
+      frame.project(params.get(), stream);
+      const int64_t K = frame.bin(true, stream);
+      frame.reserve_pairs(K + K / 2 + 65536);
+      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
+    }
+    for (int attempt = 0; attempt < 3; ++attempt) {
+      upload_scalars();
+      if (use_graph) {
+        const bool stale = g.exec == nullptr || g.N != N || g.V != frame.V ||
+                           g.timing != timing || g.pixels != b.total_pixels ||
+                           g.tiles != b.total_tiles || g.pair_capacity != frame.pair_capacity ||
+                           g.record_capacity != frame.record_capacity ||
+                           g.generation != generation ||
+                           g.raster_generation != pxs::raster_config().generation ||
+                           g.allocations != pxs::g_device_allocations;
+        if (stale) {
+          g.reset();
+          const int64_t before = pxs::g_kernel_launches;
+          PXS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+          try {
+            enqueue_batch_body(with_adam);
+          } catch (...) {
+            cudaGraph_t dropped = nullptr;
+            cudaStreamEndCapture(stream, &dropped);
+            if (dropped) cudaGraphDestroy(dropped);
+            throw;
+          }
+          PXS_CUDA(cudaStreamEndCapture(stream, &g.graph));
+          PXS_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+          g.N = N;
+          g.V = frame.V;
+          g.pixels = b.total_pixels;
+          g.tiles = b.total_tiles;
+          g.pair_capacity = frame.pair_capacity;
+          g.record_capacity = frame.record_capacity;
+          g.generation = generation;
+          g.raster_generation = pxs::raster_config().generation;
+          g.allocations = pxs::g_device_allocations;
+          g.timing = timing;
+          g.launches = pxs::g_kernel_launches - before;
+        }
+        PXS_CUDA(cudaGraphLaunch(g.exec, stream));
+        last_launches = g.launches;
+      } else {
+        const int64_t before = pxs::g_kernel_launches;
+        enqueue_batch_body(with_adam);
+        last_launches = pxs::g_kernel_launches - before;
+      }
+      PXS_CUDA(cudaStreamSynchronize(stream));
+      if (*host_overflow == 0) {
+        collect_timing();
+        PXS_CUDA(cudaMemcpy(&last_pairs, frame.d_total_pairs.get(), sizeof(int64_t),
+                            cudaMemcpyDeviceToHost));
+        return;
+      }
+      // the pairs did not fit: nothing of this step counts; grow and redo
+      PXS_CUDA(cudaMemsetAsync(grads.get(), 0, sizeof(float) * P * std::max(N, 1), stream));
+      PXS_CUDA(cudaMemsetAsync(screen_gradient.get(), 0, sizeof(float) * std::max(N, 1), stream));
+      PXS_CUDA(cudaMemsetAsync(visible_count.get(), 0, sizeof(int32_t) * std::max(N, 1), stream));
+      frame.project(params.get(), stream);
+      const int64_t K = frame.bin(true, stream);
+      frame.reserve_pairs(K + K / 2 + 65536);
+      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
+      g.reset();
+    }
+    throw Error(PXS_ERR_CAPACITY, "tile pairs overflowed three times");
   }
 
   // Times the compositing kernels with 1, 2 and 4 pixels per thread on one
@@ -449,81 +532,36 @@ struct pxs_trainer {
   float step_batch(int n_views, const int32_t* ids, bool use_graph) {
     if (schedule_done()) return 0.f;
     const std::vector<int> views = take_views(n_views, ids);
-    const pxs::ViewBatch b = batch_for(views);
-    frame.prepare(b, N, S, stream);  // also uploads the view descriptors
-    dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
-    if (frame.pair_capacity == 0 || frame.record_capacity == 0) {
-      // learn the pair count once, then run unsynchronised with headroom
-      frame.project(params.get(), stream);
-      const int64_t K = frame.bin(true, stream);
-      frame.reserve_pairs(K + K / 2 + 65536);
-      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
-    }
-    for (int attempt = 0; attempt < 3; ++attempt) {
-      upload_scalars();
-      if (use_graph) {
-        const bool stale = graph.exec == nullptr || graph.N != N || graph.V != frame.V ||
-                           graph.timing != timing ||
-                           graph.pixels != b.total_pixels || graph.tiles != b.total_tiles ||
-                           graph.pair_capacity != frame.pair_capacity ||
-                           graph.record_capacity != frame.record_capacity ||
-                           graph.generation != generation ||
-                           graph.raster_generation != pxs::raster_config().generation ||
-                           graph.allocations != pxs::g_device_allocations;
-        if (stale) {
-          graph.reset();
-          const int64_t before = pxs::g_kernel_launches;
-          PXS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-          try {
-            enqueue_batch_body();
-          } catch (...) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(stream, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-          }
-          PXS_CUDA(cudaStreamEndCapture(stream, &graph.graph));
-          PXS_CUDA(cudaGraphInstantiate(&graph.exec, graph.graph, 0));
-          graph.N = N;
-          graph.V = frame.V;
-          graph.pixels = b.total_pixels;
-          graph.tiles = b.total_tiles;
-          graph.pair_capacity = frame.pair_capacity;
-          graph.record_capacity = frame.record_capacity;
-          graph.generation = generation;
-          graph.raster_generation = pxs::raster_config().generation;
-          graph.allocations = pxs::g_device_allocations;
-          graph.timing = timing;
-          graph.launches = pxs::g_kernel_launches - before;
-        }
-        PXS_CUDA(cudaGraphLaunch(graph.exec, stream));
-        last_launches = graph.launches;
-      } else {
-        const int64_t before = pxs::g_kernel_launches;
-        enqueue_batch_body();
-        last_launches = pxs::g_kernel_launches - before;
-      }
-      PXS_CUDA(cudaStreamSynchronize(stream));
-      if (*host_overflow == 0) {
-        collect_timing();
-        PXS_CUDA(cudaMemcpy(&last_pairs, frame.d_total_pairs.get(), sizeof(int64_t),
-                            cudaMemcpyDeviceToHost));
-        break;
-      }
-      // the pairs did not fit: the optimiser skipped this step; grow and redo
-      PXS_CUDA(cudaMemsetAsync(grads.get(), 0, sizeof(float) * P * std::max(N, 1), stream));
-      PXS_CUDA(cudaMemsetAsync(screen_gradient.get(), 0, sizeof(float) * std::max(N, 1), stream));
-      PXS_CUDA(cudaMemsetAsync(visible_count.get(), 0, sizeof(int32_t) * std::max(N, 1), stream));
-      frame.project(params.get(), stream);
-      const int64_t K = frame.bin(true, stream);
-      frame.reserve_pairs(K + K / 2 + 65536);
-      frame.reserve_records(frame.last_record_count + frame.last_record_count / 2 + 65536);
-      graph.reset();
-    }
-    if (*host_overflow != 0) throw Error(PXS_ERR_CAPACITY, "tile pairs overflowed three times");
+    run_batch(views, use_graph, true, graph);
     record_loss(*host_loss);
     after_step();
     return *host_loss;
+  }
+
+  // The data-parallel split of step_batch. accumulate() renders and
+  // differentiates this rank's views and leaves the summed gradients, screen
+  // gradients and visible counts in the trainer's buffers, with no optimiser
+  // step; the caller sums those buffers over the ranks; apply() then takes
+  // the Adam step (and the schedule's densify and opacity reset) with the
+  // summed gradients and records `loss`, the mean over all ranks' views.
+  // Ranks that apply the same sums stay identical.
+  float accumulate(int n_views, const int32_t* ids, bool use_graph) {
+    if (schedule_done()) throw Error(PXS_ERR_INVALID, "the schedule is finished");
+    if (pending_apply) throw Error(PXS_ERR_INVALID, "accumulate twice without apply");
+    const std::vector<int> views = take_views(n_views, ids);
+    run_batch(views, use_graph, false, graph_acc);
+    pending_apply = true;
+    return *host_loss;
+  }
+
+  void apply(float loss) {
+    if (!pending_apply) throw Error(PXS_ERR_INVALID, "apply without accumulate");
+    upload_scalars();
+    adam();
+    PXS_CUDA(cudaStreamSynchronize(stream));
+    pending_apply = false;
+    record_loss(loss);
+    after_step();
   }
 };
 
@@ -684,6 +722,30 @@ int pxs_trainer_step_batch(pxs_trainer* t, int32_t n_views, const int32_t* view_
   });
 }
 
+int pxs_trainer_accumulate(pxs_trainer* t, int32_t n_views, const int32_t* view_ids,
+                           int32_t use_graph, float* loss) {
+  return guarded(t, [&] {
+    if (n_views <= 0) throw Error(PXS_ERR_INVALID, "n_views must be positive");
+    const float l = t->accumulate(n_views, view_ids, use_graph != 0);
+    if (loss) *loss = l;
+  });
+}
+
+int pxs_trainer_apply(pxs_trainer* t, float loss) {
+  return guarded(t, [&] { t->apply(loss); });
+}
+
+int pxs_trainer_gradients(pxs_trainer* t, float** params, float** screen_gradient,
+                          int32_t** visible_count, int32_t* count, int32_t* values) {
+  return guarded(t, [&] {
+    if (params) *params = t->grads.get();
+    if (screen_gradient) *screen_gradient = t->screen_gradient.get();
+    if (visible_count) *visible_count = t->visible_count.get();
+    if (count) *count = t->N;
+    if (values) *values = t->P;
+  });
+}
+
 int pxs_trainer_autotune(pxs_trainer* t, int32_t n_views, const int32_t* view_ids,
                          int32_t* forward_px, int32_t* backward_px) {
   return guarded(t, [&] {
@@ -711,6 +773,7 @@ int pxs_trainer_render(pxs_trainer* t, const pxs_camera* camera,
     const pxs_raster_options opt = options != nullptr ? *options : t->options();
     const pxs::ViewBatch b = pxs::make_batch(camera, 1, opt, t->cloud_sh);
     t->graph.reset();  // the frame's buffers may be resized
+    t->graph_acc.reset();
     t->frame.prepare(b, t->N, t->S, t->stream);
     t->frame.project(t->params.get(), t->stream);
     t->frame.bin(true, t->stream);

@@ -347,6 +347,36 @@ class SplatTrainer:
                                                      ct.byref(loss)))
         return loss.value
 
+    def accumulate(self, view_ids: Sequence[int], graph: bool = True) -> float:
+        """The first half of a data-parallel step: gradients of these views into
+        the device buffers, no optimiser step. Returns their mean loss."""
+        n = len(view_ids)
+        ids = (ct.c_int32 * n)(*view_ids)
+        loss = ct.c_float()
+        self._check(self._lib.pxs_trainer_accumulate(self.handle, n, ids, int(graph),
+                                                     ct.byref(loss)))
+        return loss.value
+
+    def apply(self, loss: float) -> None:
+        """The second half: the Adam step with the (summed) gradient buffers."""
+        self._check(self._lib.pxs_trainer_apply(self.handle, ct.c_float(loss)))
+
+    def gradient_buffers(self):
+        """Device pointers of the gradient buffers that a data-parallel step sums
+        over ranks: [(pointer, element count, 'float32' | 'int32'), ...]."""
+        g, sg, vc = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        n, P = ct.c_int32(), ct.c_int32()
+        self._check(self._lib.pxs_trainer_gradients(self.handle, ct.byref(g), ct.byref(sg),
+                                                    ct.byref(vc), ct.byref(n), ct.byref(P)))
+        return [(g.value, P.value * n.value, "float32"), (sg.value, n.value, "float32"),
+                (vc.value, n.value, "int32")]
+
+    def stream(self) -> int:
+        """The trainer's CUDA stream (a cudaStream_t as an integer)."""
+        sp = ct.c_void_p()
+        self._check(self._lib.pxs_trainer_stream(self.handle, ct.byref(sp)))
+        return sp.value or 0
+
     def step_views(self, n_views: int, view_ids: Optional[Sequence[int]] = None) -> float:
         """Plain multi-view step (per-view kernel sequences, host-synchronised)."""
         ids = None if view_ids is None else (ct.c_int32 * n_views)(*view_ids)
