@@ -98,14 +98,23 @@ struct RasterConfig {
 };
 RasterConfig& raster_config();
 
-void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+// The forward pass; with two pixels per thread and `block_bits` given it also
+// writes, per tile-list entry, a byte whose bit b is set when some pixel of
+// the tile's 8x8 block b (b = 2 * row block + column block) took the entry.
+// Returns whether it wrote them.
+bool launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
-                    cudaStream_t stream, unsigned long long* counts = nullptr);
+                    cudaStream_t stream, unsigned long long* counts = nullptr,
+                    uint8_t* block_bits = nullptr);
+// The adjoint. `block_bits`, when the forward wrote them, replace the
+// geometric warp masks in the two-pixel form: a warp walks only the entries
+// one of its pixels took.
 void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                      const float4* conic_op, const float4* color, const ViewDesc* views,
                      int n_views, int total_tiles, const float* T_final, const int32_t* last,
-                     const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream);
+                     const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream,
+                     const uint8_t* block_bits = nullptr);
 
 // loss.cu
 size_t loss_smem_bytes();

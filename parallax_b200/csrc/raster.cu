@@ -153,12 +153,14 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,
                  int n_views, float* __restrict__ rgb_out, float* __restrict__ T_out,
-                 int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts) {
+                 int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts,
+                 uint8_t* __restrict__ block_bits) {
   constexpr int kThreads = TileGeom<2>::kThreads;
   __shared__ float2 s_xy[kBatch];
   __shared__ float4 s_co[kBatch];
   __shared__ float4 s_col[kBatch];  // r, g, b, power floor
   __shared__ uint32_t s_mask[kBatch];
+  __shared__ uint8_t s_took[TileGeom<2>::kWarps][kBatch];  // warp w = 8x8 block w
   const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
   const int warp = threadIdx.x >> 5;
   const ViewDesc& vd = views[info.view];
@@ -172,10 +174,27 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
   float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
   int last0 = info.range.x, last1 = info.range.x;
   unsigned long long evaluated = 0, contributing = 0;
+  int prev_base = 0, prev_n = 0;  // the batch whose block bits are pending
+  // block bits of the pending batch out to global memory, one byte per entry
+  auto write_bits = [&]() {
+    for (int i = threadIdx.x; i < prev_n; i += kThreads)
+      block_bits[prev_base + i] = (uint8_t)(s_took[0][i] | (s_took[1][i] << 1) |
+                                            (s_took[2][i] << 2) | (s_took[3][i] << 3));
+  };
   for (int base = info.range.x; base < info.range.y; base += kBatch) {
-    if (__syncthreads_and(done0 && done1)) break;
+    const bool all_done = __syncthreads_and(done0 && done1);
+    if (block_bits != nullptr) {
+      write_bits();
+      prev_n = 0;
+    }
+    if (all_done) break;
+    if (block_bits != nullptr) __syncthreads();  // the bits are read before they are cleared
     const int n = min(kBatch, info.range.y - base);
     for (int i = threadIdx.x; i < n; i += kThreads) {
+      if (block_bits != nullptr) {
+#pragma unroll
+        for (int w = 0; w < TileGeom<2>::kWarps; ++w) s_took[w][i] = 0;
+      }
       const uint32_t slot = pair_slots[base + i];
       const float4 co = conic_op[slot];
       const float2 mean = xy[slot];
@@ -208,6 +227,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
         const bool c1 = in1 && !(a1 < min_alpha);
         if (!(c0 || c1)) continue;
         if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
+        if (block_bits != nullptr) s_took[warp][j] = 1;  // same value from every lane
         const float4 c = s_col[j];
         const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
         acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
@@ -226,6 +246,12 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
         if (done0 && done1) break;
       }
     }
+    prev_base = base;
+    prev_n = n;
+  }
+  if (block_bits != nullptr && prev_n > 0) {  // the last batch, when the list ran out
+    __syncthreads();
+    write_bits();
   }
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
@@ -267,7 +293,7 @@ template <bool kCount>
 void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                       const float4* conic_op, const float4* color, const ViewDesc* views,
                       int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
-                      cudaStream_t stream, unsigned long long* counts) {
+                      cudaStream_t stream, unsigned long long* counts, uint8_t* bits) {
   switch (px) {
     case 1:
       forward_px<kCount, 1>(ranges, pair_slots, xy, conic_op, color, views, n_views,
@@ -279,25 +305,27 @@ void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, co
       break;
     default:
       k_forward_x2<kCount><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts);
+          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts, bits);
   }
 }
 
 }  // namespace
 
-void launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+bool launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
-                    cudaStream_t stream, unsigned long long* counts) {
-  if (total_tiles <= 0) return;
+                    cudaStream_t stream, unsigned long long* counts, uint8_t* block_bits) {
+  if (total_tiles <= 0) return false;
   count_launch();
   const int px = raster_config().forward_px;
+  uint8_t* bits = (px == 1 || px == 4) ? nullptr : block_bits;
   if (counts != nullptr)
     forward_dispatch<true>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
-                           total_tiles, rgb, T, last, stream, counts);
+                           total_tiles, rgb, T, last, stream, counts, bits);
   else
     forward_dispatch<false>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
-                            total_tiles, rgb, T, last, stream, nullptr);
+                            total_tiles, rgb, T, last, stream, nullptr, bits);
+  return bits != nullptr;
 }
 
 }  // namespace pxs

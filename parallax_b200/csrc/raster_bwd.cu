@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
                   const float4* __restrict__ color, const ViewDesc* __restrict__ views,
                   int n_views, const float* __restrict__ T_final,
                   const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
-                  ScreenGrad* __restrict__ screen) {
+                  ScreenGrad* __restrict__ screen, const uint8_t* __restrict__ block_bits) {
   constexpr int kThreads = TileGeom<2>::kThreads;
   __shared__ uint32_t s_slot[kBatch];
   __shared__ float2 s_xy[kBatch];
@@ -309,14 +309,18 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
       s_xy[i] = mean;
       s_co[i] = co;
       s_col[i] = c;
-      s_mask[i] = warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
+      // which warps took the entry in the forward pass (exact), else which
+      // ones its footprint can reach
+      s_mask[i] = block_bits != nullptr
+                      ? (uint32_t)block_bits[batch_start + i]
+                      : warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
 #pragma unroll
       for (int k = 0; k < 12; ++k) s_acc[i][k] = 0.f;
     }
     __syncthreads();
     const int j_top = min(n, warp_hi - batch_start) - 1;  // warp-uniform
     for (int j = j_top; j >= 0; --j) {
-      if (!((s_mask[j] >> warp) & 1u)) continue;  // cannot reach this warp's pixels
+      if (!((s_mask[j] >> warp) & 1u)) continue;  // no pixel of this warp takes it
       const int e = batch_start + j;
       const float2 m = s_xy[j];
       const float4 co = s_co[j];
@@ -458,7 +462,8 @@ void backward_px(const int2* ranges, const uint32_t* pair_slots, const float2* x
 void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                      const float4* conic_op, const float4* color, const ViewDesc* views,
                      int n_views, int total_tiles, const float* T_final, const int32_t* last,
-                     const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream) {
+                     const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream,
+                     const uint8_t* block_bits) {
   if (total_tiles <= 0) return;
   count_launch();
   switch (raster_config().backward_px) {
@@ -473,7 +478,7 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
     default:
       k_backward_x2<<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
           ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
-          screen);
+          screen, block_bits);
   }
 }
 

@@ -145,6 +145,7 @@ void Frame::reserve_pairs(int64_t capacity) {
   if (capacity <= pair_capacity && tile_slots.get() != nullptr) return;
   const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
   tile_slots.reserve(cap);
+  block_bits.reserve(cap);
   pair_capacity = static_cast<int64_t>(cap);
 }
 
@@ -262,9 +263,10 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
 }
 
 void Frame::forward(cudaStream_t stream, unsigned long long* counts) {
-  launch_forward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
-                 d_views.get(), V, batch.total_tiles, rgb.get(), transmittance.get(), last.get(),
-                 stream, counts);
+  have_block_bits =
+      launch_forward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
+                     d_views.get(), V, batch.total_tiles, rgb.get(), transmittance.get(),
+                     last.get(), stream, counts, block_bits.get());
   PXS_CUDA(cudaGetLastError());
 }
 
@@ -284,7 +286,7 @@ void Frame::backward(const float* dL_drgb, cudaStream_t stream) {
   PXS_CUDA(cudaMemsetAsync(screen.get(), 0, sizeof(ScreenGrad) * slots, stream));
   launch_backward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
                   d_views.get(), V, batch.total_tiles, transmittance.get(), last.get(), dL_drgb,
-                  screen.get(), stream);
+                  screen.get(), stream, have_block_bits ? block_bits.get() : nullptr);
   PXS_CUDA(cudaGetLastError());
 }
 

@@ -150,6 +150,10 @@ class Frame {
   int64_t max_chunks = 0;
   DeviceArray<int64_t> tile_offsets;
   DeviceArray<uint32_t> tile_slots;  // per-tile key lists (pair_capacity)
+  // per list entry, which 8x8 blocks of its tile took it (pair_capacity bytes),
+  // written by the two-pixel forward pass for its adjoint
+  DeviceArray<uint8_t> block_bits;
+  bool have_block_bits = false;
   DeviceArray<uint32_t> hist, hist_scanned;
   DeviceArray<char> scan_scratch;
   DeviceArray<int2> ranges;
