@@ -358,9 +358,10 @@ int pxs_get_raster_config(int32_t* forward_px, int32_t* backward_px);
 
 /* The autotuner: times the compositing kernel and its adjoint with 1, 2 and
  * 4 pixels per thread on the batch of `view_ids` (NULL: the first n_views
- * views) and keeps the fastest of each (written to forward_px / backward_px,
- * either may be NULL). The schedule, the cloud and its gradients are not
- * changed. */
+ * views) and keeps the fastest forward + adjoint pair, timed together (the
+ * two-pixel forward records which 8x8 blocks took each entry, which the
+ * two-pixel adjoint uses), written to forward_px / backward_px (either may be
+ * NULL). The schedule, the cloud and its gradients are not changed. */
 int pxs_trainer_autotune(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                          int32_t* forward_px, int32_t* backward_px);
 

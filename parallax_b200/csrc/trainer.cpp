@@ -461,7 +461,7 @@ struct pxs_trainer {
   }
 
   // Times the compositing kernels with 1, 2 and 4 pixels per thread on one
-  // batch of views and keeps the fastest forward and the fastest backward.
+  // batch of views and keeps the fastest forward + backward pair.
   // The schedule, the parameters and the gradients are left as they were.
   void autotune(int n_views, const int32_t* ids, int* forward_px, int* backward_px) {
     std::vector<int> views;
@@ -491,26 +491,25 @@ struct pxs_trainer {
     };
     pxs::RasterConfig& rc = pxs::raster_config();
     const int candidates[3] = {1, 2, 4};
+    // the pair is timed together: the two-pixel forward also records which
+    // blocks took each entry, which the two-pixel adjoint then skips by
     float best = 0.f;
+    bool have_best = false;
     int best_fwd = rc.forward_px, best_bwd = rc.backward_px;
     try {
-      for (int px : candidates) {
-        rc.forward_px = px;
-        const float ms = time_ms([&] { frame.forward(stream); });
-        if (px == candidates[0] || ms < best) {
-          best = ms;
-          best_fwd = px;
-        }
-      }
-      rc.forward_px = best_fwd;
-      frame.forward(stream);
-      frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
-      for (int px : candidates) {
-        rc.backward_px = px;
-        const float ms = time_ms([&] { frame.backward(d_dL, stream); });
-        if (px == candidates[0] || ms < best) {
-          best = ms;
-          best_bwd = px;
+      for (int fpx : candidates) {
+        rc.forward_px = fpx;
+        const float f_ms = time_ms([&] { frame.forward(stream); });
+        frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
+        for (int bpx : candidates) {
+          rc.backward_px = bpx;
+          const float ms = f_ms + time_ms([&] { frame.backward(d_dL, stream); });
+          if (!have_best || ms < best) {
+            best = ms;
+            best_fwd = fpx;
+            best_bwd = bpx;
+            have_best = true;
+          }
         }
       }
     } catch (...) {
