@@ -530,6 +530,87 @@ def run_ours(args):
         print(json.dumps(line))
 
 
+def run_multi_scene(args):
+    """The uneven batch of independent scans: 32 scenes (5k-150k gaussians SH3,
+    320x240 / 640x480 / 1280x720), 4 views each; one step renders and
+    differentiates all 128 views in one pass of each kernel and takes every
+    scene's Adam step (a multi-scene trainer, pxs_trainer_create_scenes)."""
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    import parallax_b200 as px
+    from parallax_b200.scenes import MULTI_SCENE, multi_scene_workload
+
+    scenes = multi_scene_workload(5)
+    lib = px.lib()
+    opts = px.RasterOptions(sh_degree=MULTI_SCENE["sh_degree"])
+    scene_views, starts = [], []
+    for truth, start, views in scenes:
+        renderer = px.SplatTrainer(truth, [], px.TrainConfig(iterations=1))
+        pairs = []
+        for view in views:
+            arr = np.empty(view.width * view.height * 3, dtype=np.float32)
+            cam = view.camera()
+            renderer._check(lib.pxs_trainer_render(renderer.handle, ct.byref(cam),
+                                                   ct.byref(opts), arr.ctypes.data, None))
+            pairs.append((cam, arr))
+        renderer.close()
+        scene_views.append(pairs)
+        starts.append(start)
+    cfg = px.TrainConfig(iterations=100000, sh_degree=MULTI_SCENE["sh_degree"],
+                         sh_increase_interval=0, densify_from_iteration=10 ** 9,
+                         densify_until_iteration=10 ** 9, opacity_reset_interval=0)
+    trainer = px.SplatTrainer.from_scenes(starts, scene_views, cfg, device=local)
+    n_views = sum(len(v) for v in scene_views)
+    ids = list(range(n_views))
+    sp = ct.c_void_p()
+    trainer._check(lib.pxs_trainer_stream(trainer.handle, ct.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    fpx, bpx = ct.c_int32(), ct.c_int32()
+    id_arr = (ct.c_int32 * n_views)(*ids)
+    trainer._check(lib.pxs_trainer_autotune(trainer.handle, n_views, id_arr, ct.byref(fpx),
+                                            ct.byref(bpx)))
+    for _ in range(max(args.warmup, 3)):
+        trainer.step_batch(n_views, ids)
+    trainer._check(lib.pxs_trainer_set_timing(trainer.handle, 1))
+    trainer.step_batch(n_views, ids)
+    trainer._check(lib.pxs_trainer_set_timing(trainer.handle, 1))
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        trainer.step_batch(n_views, ids)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    stage_ms = (ct.c_float * len(STAGES))()
+    n_stages, n_steps = ct.c_int32(), ct.c_int32()
+    trainer._check(lib.pxs_trainer_stage_times(trainer.handle, stage_ms, len(STAGES),
+                                               ct.byref(n_stages), ct.byref(n_steps)))
+    pairs, launches = ct.c_int64(), ct.c_int64()
+    trainer._check(lib.pxs_trainer_step_info(trainer.handle, ct.byref(pairs), ct.byref(launches)))
+    counts = [c.count for c in starts]
+    line = {
+        "metric": "train steps/s (fwd+bwd+Adam), 32 independent scenes x 4 views in one "
+                  "batched graph-captured step",
+        "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded: scene s truth cloud 1000+2s, start 1001+2s, cameras 3000+s)",
+        "config": {"workload": f"c5: {len(starts)} scenes, {sum(counts)} gaussians "
+                               f"({min(counts)}..{max(counts)}) SH{MULTI_SCENE['sh_degree']}, "
+                               f"{n_views} views of 320x240 / 640x480 / 1280x720",
+                   "pixels_per_thread": {"forward": fpx.value, "backward": bpx.value}},
+        "gpu_launches": launches.value * args.steps, "kernels_per_step": launches.value,
+        "pairs_per_step": pairs.value,
+        "stage_ms": {s: stage_ms[i] / max(n_steps.value, 1) for i, s in enumerate(STAGES)},
+    }
+    trainer.close()
+    print(json.dumps(line))
+
+
 def traffic_from_profiles(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -596,6 +677,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c5":
+        run_multi_scene(args)
     else:
         run_ours(args)
 

@@ -318,6 +318,25 @@ int pxs_trainer_train(pxs_trainer* trainer, pxs_progress_fn callback, void* user
 int pxs_trainer_step_batch(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                            int32_t graph, float* loss);
 
+/* A trainer over several independent scenes in one cloud, for batches that
+ * render and differentiate views of many scenes of uneven sizes in one pass
+ * of each kernel. Scene s has its own cloud (clouds[s]; all with the same
+ * rest_per_channel and sh_degree) and views_per_scene[s] consecutive entries
+ * of cameras / images. The scenes are joined into one cloud (scene after
+ * scene, component-major), every view renders only its own scene's
+ * gaussians, and the position learning rate of each gaussian uses its own
+ * scene's camera extent (positionLearningRate, SplatTrainer.cpp:200-208), so a
+ * step over a batch of views updates every scene as its own trainer would.
+ * Train with pxs_trainer_step_batch / step_views / accumulate; read the
+ * result with pxs_trainer_download (the joined cloud, scene after scene).
+ * Densification resizes one cloud, so with more than one scene the config
+ * must not densify (densify_from_iteration past the last iteration), and
+ * pxs_trainer_finish is refused. */
+int pxs_trainer_create_scenes(const pxs_train_config* config, const pxs_cloud* clouds,
+                              int32_t n_scenes, const int32_t* views_per_scene,
+                              const pxs_camera* cameras, const float* const* images,
+                              int32_t device, pxs_trainer** trainer);
+
 /* The data-parallel split of pxs_trainer_step_batch, for one trainer per GPU
  * over a shared cloud. pxs_trainer_accumulate renders and differentiates this
  * rank's `n_views` views (a graph replay when `graph` is nonzero) and leaves

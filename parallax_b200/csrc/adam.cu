@@ -24,7 +24,8 @@ __global__ void __launch_bounds__(256)
            float* __restrict__ v, int N, int S, const StepScalars* __restrict__ scalars,
            int zero_grads, float* __restrict__ screen_gradient,
            int32_t* __restrict__ visible_count, float* __restrict__ acc_gradient,
-           int32_t* __restrict__ acc_views, const int32_t* __restrict__ skip) {
+           int32_t* __restrict__ acc_views, const int32_t* __restrict__ skip,
+           const float* __restrict__ position_scale) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= N) return;
   // a step whose tile pairs overflowed is redone by the host: leave the state alone
@@ -32,13 +33,16 @@ __global__ void __launch_bounds__(256)
   const StepScalars& s = *scalars;
   const int64_t n = N;
   const int P = 14 + 3 * S;
+  // positionLearningRate (SplatTrainer.cpp:200-208) ends with "* extent": with
+  // several scenes lr[0] holds the rest and each gaussian its scene's extent
+  const float lr_position = position_scale != nullptr ? s.lr[0] * position_scale[g] : s.lr[0];
   for (int c = 0; c < P; ++c) {
     if (c >= PXS_C_ROTATION && c < PXS_C_ROTATION + 4) continue;
     const int group = c < 3 ? 0 : (c < 6 ? 1 : (c == PXS_C_OPACITY ? 3 : (c < 14 ? 4 : 5)));
     const int64_t i = (int64_t)c * n + g;
     float mm = m[i], vv = v[i];
-    params[i] += adam_delta(mm, vv, grads[i], s.lr[group], s.beta1, s.beta2, s.epsilon,
-                            s.correction1, s.correction2);
+    params[i] += adam_delta(mm, vv, grads[i], group == 0 ? lr_position : s.lr[group], s.beta1,
+                            s.beta2, s.epsilon, s.correction1, s.correction2);
     m[i] = mm;
     v[i] = vv;
     if (zero_grads) grads[i] = 0.f;
@@ -82,23 +86,24 @@ __global__ void __launch_bounds__(256)
 void launch_adam(float* params, float* grads, float* m, float* v, int N, int S,
                  const StepScalars* scalars, int zero_grads, float* screen_gradient,
                  int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, const float* position_scale) {
   if (N <= 0) return;
   count_launch();
   k_adam<<<(N + 255) / 256, 256, 0, stream>>>(params, grads, m, v, N, S, scalars, zero_grads,
                                               screen_gradient, visible_count, acc_gradient,
-                                              acc_views, nullptr);
+                                              acc_views, nullptr, position_scale);
 }
 
 void launch_adam_checked(float* params, float* grads, float* m, float* v, int N, int S,
                          const StepScalars* scalars, float* screen_gradient,
                          int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
-                         const int32_t* skip, cudaStream_t stream) {
+                         const int32_t* skip, cudaStream_t stream,
+                         const float* position_scale) {
   if (N <= 0) return;
   count_launch();
   k_adam<<<(N + 255) / 256, 256, 0, stream>>>(params, grads, m, v, N, S, scalars, 1,
                                               screen_gradient, visible_count, acc_gradient,
-                                              acc_views, skip);
+                                              acc_views, skip, position_scale);
 }
 
 // resetOpacity (SplatTrainer.cpp:301-309): cap the logit, clear its moments.

@@ -39,6 +39,12 @@ struct ViewDesc {
   float screen_dilation;
   int32_t pad1;
   int64_t target_offset;     // first pixel of this view's target image
+  // the gaussians this view renders: [gauss_offset, gauss_offset + gauss_count)
+  // of the parameter arrays; slot v * slot_stride + i holds gaussian
+  // gauss_offset + i (one cloud: 0 and N for every view; a batch of several
+  // independent scenes: each view's own scene)
+  int32_t gauss_offset;
+  int32_t gauss_count;
 };
 
 // Per-step screen-space gradient accumulators of one (view, gaussian) slot

@@ -127,15 +127,18 @@ void launch_loss(const float* rendered, const float* target, const ViewDesc* vie
 float measure_fp32_peak_tflops(cudaStream_t stream);
 
 // adam.cu
+// `position_scale` (N floats, optional) multiplies the position learning rate
+// per gaussian: each scene's extent, when one cloud holds several scenes.
 void launch_adam(float* params, float* grads, float* m, float* v, int N, int S,
                  const StepScalars* scalars, int zero_grads, float* screen_gradient,
                  int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
-                 cudaStream_t stream);
+                 cudaStream_t stream, const float* position_scale = nullptr);
 // Same step, skipped entirely when *skip is nonzero (a batch whose pairs overflowed).
 void launch_adam_checked(float* params, float* grads, float* m, float* v, int N, int S,
                          const StepScalars* scalars, float* screen_gradient,
                          int32_t* visible_count, float* acc_gradient, int32_t* acc_views,
-                         const int32_t* skip, cudaStream_t stream);
+                         const int32_t* skip, cudaStream_t stream,
+                         const float* position_scale = nullptr);
 void launch_reset_opacity(float* params, float* m, float* v, int N, float ceiling,
                           cudaStream_t stream);
 

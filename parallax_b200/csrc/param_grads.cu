@@ -2,8 +2,10 @@
 // screen-space gradients back to each gaussian's parameters.
 //
 // rasterizeSplatsBackward, parameter pass (SplatRaster.cpp:435-575). One
-// thread per gaussian loops over the batch's views, keeping the parameter
-// gradients in registers, and adds them into the gradient array once. The
+// thread per gaussian loops over the batch's views that render it (every
+// view for one cloud; its scene's views for a batch of several scenes),
+// keeping the parameter gradients in registers, and adds them into the
+// gradient array once. The
 // chain is gradient arithmetic, compiled with fused multiply-adds.
 #include "common.cuh"
 #include "kernels.h"
@@ -98,7 +100,9 @@ __global__ void __launch_bounds__(128, 3)
   float pos[3] = {0.f, 0.f, 0.f}, qn[4] = {1.f, 0.f, 0.f, 0.f}, sc[3] = {0.f, 0.f, 0.f};
 
   for (int v = 0; v < n_views; ++v) {
-    const int64_t slot = v * slot_stride + g;
+    const int local = g - views[v].gauss_offset;  // this gaussian's slot in view v, if any
+    if (local < 0 || local >= views[v].gauss_count) continue;
+    const int64_t slot = v * slot_stride + local;
     if (depth_key[slot] == kCulledKey) continue;
     const ScreenGrad sg = screen[slot];
     visible += 1;

@@ -14,30 +14,35 @@
 namespace pxs {
 
 
-// One thread per gaussian, looping over the views of the batch so the
-// parameters are read once (projectSplats, SplatRaster.cpp:201-258).
+// One thread per slot index i, looping over the views of the batch: view v's
+// slot i holds gaussian gauss_offset + i of that view's range. Views of one
+// cloud share the gaussian, so its parameters are read once; a batch of
+// several scenes reads each scene's gaussian when the scene changes
+// (projectSplats, SplatRaster.cpp:201-258).
 __global__ void __launch_bounds__(256)
     k_project(const float* __restrict__ params, int N, int S, int64_t slot_stride,
               const ViewDesc* __restrict__ views, int n_views, ProjectedSoA out) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= slot_stride) return;
-  if (g >= N) {
-    for (int v = 0; v < n_views; ++v) {
-      const int64_t slot = v * slot_stride + g;
-      out.depth_key[slot] = kCulledKey;
-      out.tile_count[slot] = 0;
-    }
-    return;
-  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slot_stride) return;
   GaussianState st;
-  load_state(params, N, g, st);
-  const float dc0 = params[(int64_t)(PXS_C_DC + 0) * N + g];
-  const float dc1 = params[(int64_t)(PXS_C_DC + 1) * N + g];
-  const float dc2 = params[(int64_t)(PXS_C_DC + 2) * N + g];
+  int g = -1;  // the gaussian whose state is loaded
+  float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
 
   for (int v = 0; v < n_views; ++v) {
-    const int64_t slot = v * slot_stride + g;
+    const int64_t slot = v * slot_stride + i;
     const ViewDesc& vd = views[v];
+    if (i >= vd.gauss_count) {
+      out.depth_key[slot] = kCulledKey;
+      out.tile_count[slot] = 0;
+      continue;
+    }
+    if (vd.gauss_offset + i != g) {
+      g = vd.gauss_offset + i;
+      load_state(params, N, g, st);
+      dc0 = params[(int64_t)(PXS_C_DC + 0) * N + g];
+      dc1 = params[(int64_t)(PXS_C_DC + 1) * N + g];
+      dc2 = params[(int64_t)(PXS_C_DC + 2) * N + g];
+    }
     const pxs_camera& cam = vd.cam;
     float p[3];
 #pragma unroll

@@ -91,7 +91,18 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   N = n;
   S = s;
   V = static_cast<int>(b.views.size());
-  slot_stride = round_up(std::max(N, 1), kSortTile);
+  int widest = 1;  // the largest gaussian range of a view
+  for (ViewDesc& d : batch.views) {
+    if (!batch.own_ranges) {
+      d.gauss_offset = 0;
+      d.gauss_count = N;
+    } else if (d.gauss_offset < 0 || d.gauss_count < 0 ||
+               static_cast<int64_t>(d.gauss_offset) + d.gauss_count > N) {
+      throw Error(PXS_ERR_INVALID, "a view's gaussian range lies outside the cloud");
+    }
+    widest = std::max(widest, d.gauss_count);
+  }
+  slot_stride = round_up(widest, kSortTile);
   const size_t slots = static_cast<size_t>(V) * static_cast<size_t>(slot_stride);
   d_views.reserve(static_cast<size_t>(std::max(V, 1)));
   if (V > 0)

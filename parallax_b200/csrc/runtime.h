@@ -94,6 +94,9 @@ struct ViewBatch {
   int total_rows = 0;       // tile rows over all views
   int max_tiles_x = 0;
   int max_width = 0, max_height = 0;
+  // the views carry their own gaussian ranges (several scenes); otherwise
+  // Frame::prepare gives every view the whole cloud
+  bool own_ranges = false;
 };
 
 ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_options& options,

@@ -68,6 +68,14 @@ struct pxs_trainer {
 
   int iteration = 0;
   float extent = 1.f, last_loss = 0.f, smoothed_loss = 0.f;
+  // several independent scenes in one cloud (pxs_trainer_create_scenes): the
+  // gaussian range and camera extent of each scene, the scene of each view,
+  // and per gaussian its scene's extent for the position learning rate
+  int n_scenes = 1;
+  std::vector<int32_t> scene_offset, scene_count;
+  std::vector<int> view_scene;
+  std::vector<float> scene_extent;
+  DeviceArray<float> position_scale;
   std::mt19937 engine;
   std::vector<int> order;
   size_t cursor = 0;
@@ -120,8 +128,12 @@ struct pxs_trainer {
                         ? 1.f
                         : static_cast<float>(iteration) / static_cast<float>(cfg.iterations - 1);
     const float ratio = cfg.position_lr_final / std::max(cfg.position_lr_initial, 1e-30f);
-    return cfg.position_lr_initial * std::pow(ratio, std::clamp(t, 0.f, 1.f)) * extent;
+    const float base = cfg.position_lr_initial * std::pow(ratio, std::clamp(t, 0.f, 1.f));
+    // several scenes: the Adam kernel multiplies by each gaussian's scene extent
+    return n_scenes > 1 ? base : base * extent;
   }
+
+  const float* position_scales() const { return n_scenes > 1 ? position_scale.get() : nullptr; }
 
   // nextView (SplatTrainer.cpp:210-216)
   int next_view() {
@@ -167,6 +179,14 @@ struct pxs_trainer {
                                        cloud_sh);
     for (size_t i = 0; i < ids.size(); ++i)
       b.views[i].target_offset = image_offset[static_cast<size_t>(ids[i])];
+    if (n_scenes > 1) {
+      b.own_ranges = true;
+      for (size_t i = 0; i < ids.size(); ++i) {
+        const int sc = view_scene[static_cast<size_t>(ids[i])];
+        b.views[i].gauss_offset = scene_offset[static_cast<size_t>(sc)];
+        b.views[i].gauss_count = scene_count[static_cast<size_t>(sc)];
+      }
+    }
     return b;
   }
 
@@ -178,15 +198,15 @@ struct pxs_trainer {
   void adam() {
     pxs::launch_adam(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(), 1,
                      screen_gradient.get(), visible_count.get(), acc_gradient.get(),
-                     acc_views.get(), stream);
+                     acc_views.get(), stream, position_scales());
     PXS_CUDA(cudaGetLastError());
   }
 
   // The tail of SplatTrainer::step after the optimiser (SplatTrainer.cpp:349-360).
   void after_step() {
     ++iteration;
-    if (iteration >= cfg.densify_from_iteration && iteration <= cfg.densify_until_iteration &&
-        iteration % cfg.densify_interval == 0) {
+    if (n_scenes == 1 && iteration >= cfg.densify_from_iteration &&
+        iteration <= cfg.densify_until_iteration && iteration % cfg.densify_interval == 0) {
       densify();
     }
     if (cfg.opacity_reset_interval > 0 && iteration % cfg.opacity_reset_interval == 0 &&
@@ -374,7 +394,8 @@ struct pxs_trainer {
     if (with_adam)
       pxs::launch_adam_checked(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(),
                                screen_gradient.get(), visible_count.get(), acc_gradient.get(),
-                               acc_views.get(), frame.overflow.get(), stream);
+                               acc_views.get(), frame.overflow.get(), stream,
+                               position_scales());
     mark(7);
     PXS_CUDA(cudaMemcpyAsync(host_loss, frame.loss_total.get(), sizeof(float),
                              cudaMemcpyDeviceToHost, stream));
@@ -886,6 +907,9 @@ int pxs_trainer_download(pxs_trainer* t, float* params, int32_t capacity, int32_
 
 int pxs_trainer_finish(pxs_trainer* t, float* params, int32_t capacity, int32_t* count) {
   return guarded(t, [&] {
+    if (t->n_scenes > 1)
+      throw Error(PXS_ERR_INVALID,
+                  "finish() prunes and sorts one cloud; download the scenes instead");
     ++t->generation;
     DeviceArray<float> out;
     out.reserve(static_cast<size_t>(t->P) * static_cast<size_t>(std::max(t->N, 1)));
@@ -906,6 +930,81 @@ int pxs_trainer_finish(pxs_trainer* t, float* params, int32_t capacity, int32_t*
     t->cloud_sh = t->cfg.sh_degree;
     t->iteration = t->cfg.iterations;
   });
+}
+
+int pxs_trainer_create_scenes(const pxs_train_config* config, const pxs_cloud* clouds,
+                              int32_t n_scenes, const int32_t* views_per_scene,
+                              const pxs_camera* cameras, const float* const* images,
+                              int32_t device, pxs_trainer** out) {
+  if (out == nullptr || config == nullptr || clouds == nullptr || views_per_scene == nullptr ||
+      n_scenes <= 0)
+    return PXS_ERR_INVALID;
+  *out = nullptr;
+  // densification resizes one cloud; several scenes train at a fixed size
+  const int last = std::min(config->densify_until_iteration, config->iterations);
+  if (n_scenes > 1 && config->densify_from_iteration <= last) return PXS_ERR_INVALID;
+  const int S = clouds[0].rest_per_channel;
+  int64_t total = 0;
+  int n_views = 0;
+  for (int s = 0; s < n_scenes; ++s) {
+    if (clouds[s].rest_per_channel != S || clouds[s].sh_degree != clouds[0].sh_degree ||
+        clouds[s].count < 0 || views_per_scene[s] < 0 ||
+        (clouds[s].count > 0 && clouds[s].params == nullptr))
+      return PXS_ERR_INVALID;
+    total += clouds[s].count;
+    n_views += views_per_scene[s];
+  }
+  if (total > INT32_MAX / 2) return PXS_ERR_INVALID;
+  // one component-major cloud holding the scenes one after another
+  const size_t P = static_cast<size_t>(PXS_PARAM_COUNT(S));
+  std::vector<float> joined;
+  try {
+    joined.resize(P * static_cast<size_t>(total));
+  } catch (const std::bad_alloc&) {
+    return PXS_ERR_NO_MEMORY;
+  }
+  std::vector<int32_t> offsets;
+  int64_t at = 0;
+  for (int s = 0; s < n_scenes; ++s) {
+    offsets.push_back(static_cast<int32_t>(at));
+    const size_t n = static_cast<size_t>(clouds[s].count);
+    for (size_t c = 0; c < P; ++c)
+      std::copy(clouds[s].params + c * n, clouds[s].params + (c + 1) * n,
+                joined.begin() + static_cast<ptrdiff_t>(c * static_cast<size_t>(total) + at));
+    at += clouds[s].count;
+  }
+  pxs_cloud all{joined.data(), static_cast<int32_t>(total), S, clouds[0].sh_degree};
+  pxs_trainer* t = nullptr;
+  const int status = pxs_trainer_create(config, &all, cameras, images, n_views, device, &t);
+  if (status != PXS_OK) return status;
+  const int configured = guarded(t, [&] {
+    t->n_scenes = n_scenes;
+    t->scene_offset = offsets;
+    t->scene_count.clear();
+    t->view_scene.clear();
+    t->scene_extent.clear();
+    std::vector<float> scale(static_cast<size_t>(std::max<int64_t>(total, 1)), 1.f);
+    int view = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+      t->scene_count.push_back(clouds[s].count);
+      std::vector<pxs_camera> cams(cameras + view, cameras + view + views_per_scene[s]);
+      const float e = camera_extent(cams);  // each scene's own extent
+      t->scene_extent.push_back(e);
+      for (int i = 0; i < clouds[s].count; ++i) scale[static_cast<size_t>(offsets[s] + i)] = e;
+      for (int k = 0; k < views_per_scene[s]; ++k) t->view_scene.push_back(s);
+      view += views_per_scene[s];
+    }
+    float* d = t->position_scale.reserve(scale.size());
+    PXS_CUDA(cudaMemcpyAsync(d, scale.data(), scale.size() * sizeof(float),
+                             cudaMemcpyHostToDevice, t->stream));
+    PXS_CUDA(cudaStreamSynchronize(t->stream));
+  });
+  if (configured != PXS_OK) {
+    pxs_trainer_destroy(t);
+    return configured;
+  }
+  *out = t;
+  return PXS_OK;
 }
 
 int pxs_train_splats(pxs_cloud* cloud, const pxs_camera* cameras, const float* const* images,

@@ -85,3 +85,25 @@ def workload_scene(name: str):
     start = synthetic_cloud(2, w["gaussians"], w["sh_degree"])
     views = orbit_views(3, w["pool"], w["width"], w["height"], layout=w["layout"])
     return truth, start, views
+
+
+# Uneven batch of independent scans: 32 scenes, gaussian counts log-uniform in
+# [5k, 150k], each at a resolution drawn from three phone sizes, 4 views each.
+MULTI_SCENE = dict(scenes=32, min_count=5_000, max_count=150_000, sh_degree=3,
+                   views_per_scene=4, resolutions=((320, 240), (640, 480), (1280, 720)))
+
+
+def multi_scene_workload(seed: int = 5, **overrides):
+    """[(truth cloud, start cloud, views)] per scene, all seeded from `seed`."""
+    w = dict(MULTI_SCENE, **overrides)
+    rs = np.random.default_rng(seed)
+    lo, hi = math.log(w["min_count"]), math.log(w["max_count"])
+    scenes = []
+    for s in range(w["scenes"]):
+        count = int(round(math.exp(rs.uniform(lo, hi))))
+        width, height = w["resolutions"][int(rs.integers(len(w["resolutions"])))]
+        truth = synthetic_cloud(1000 + 2 * s, count, w["sh_degree"])
+        start = synthetic_cloud(1001 + 2 * s, count, w["sh_degree"])
+        views = orbit_views(3000 + s, w["views_per_scene"], width, height)
+        scenes.append((truth, start, views))
+    return scenes

@@ -314,6 +314,34 @@ class SplatTrainer:
             raise PxsError(status, "could not create the trainer")
         self.handle = handle
 
+    @classmethod
+    def from_scenes(cls, clouds: Sequence[GaussianCloud], scene_views,
+                    config: Optional[A.TrainConfig] = None, device: int = 0) -> "SplatTrainer":
+        """A trainer over several independent scenes (pxs_trainer_create_scenes):
+        `scene_views[s]` lists scene s's (view, image) pairs; view ids run
+        scene after scene. The scenes share one joined cloud, each view renders
+        its own scene, and with more than one scene the config must not
+        densify."""
+        self = cls.__new__(cls)
+        self._lib = lib()
+        self.config = config or A.TrainConfig()
+        self.rest = clouds[0].rest_per_channel
+        self.P = A.param_count(self.rest)
+        flat = [pair for views in scene_views for pair in views]
+        cams, self._images, ptrs = _views_to_c(flat)
+        self._clouds = [c.c_struct() for c in clouds]
+        arr = (A.Cloud * len(clouds))(*self._clouds)
+        counts = (ct.c_int32 * len(clouds))(*[len(v) for v in scene_views])
+        handle = ct.c_void_p()
+        status = self._lib.pxs_trainer_create_scenes(ct.byref(self.config), arr, len(clouds),
+                                                     counts, cams, ptrs, device,
+                                                     ct.byref(handle))
+        if status != A.PXS_OK:
+            raise PxsError(status, "could not create the multi-scene trainer")
+        self.handle = handle
+        self.scene_counts = [c.count for c in clouds]
+        return self
+
     def _check(self, status: int) -> None:
         check(status, lambda: self._lib.pxs_trainer_last_error(self.handle))
 

@@ -551,3 +551,44 @@ def test_edge_cases(ctx):
                                      offsets.ctypes.data, entries.ctypes.data, 4,
                                      ct.byref(total))
     assert status == px._abi.PXS_ERR_CAPACITY and total.value > 4
+
+
+def test_multi_scene_batch_matches_per_scene_trainers():
+    """Several independent scenes of uneven sizes and resolutions in one
+    batched step (one pass of each kernel over all views) against one trainer
+    per scene stepping its own views: same losses, same clouds within the
+    order in which the device sums gradients."""
+    specs = [(2000, 64, 48, 51), (5000, 96, 72, 52), (800, 128, 96, 53)]
+    opt = RasterOptions(sh_degree=3)
+    clouds, scene_views = [], []
+    for count, w, h, seed in specs:
+        params, rest = O.random_cloud(seed, count, 3, log_scale_mean=-3.5)
+        truth, _ = O.random_cloud(seed + 100, count, 3, log_scale_mean=-3.5)
+        views = O.orbit_views(3, w, h, seed=seed)
+        images = [px.render_splats(px.GaussianCloud(truth, 3, rest), v.camera(), opt)[0]
+                  for v in views]
+        clouds.append(px.GaussianCloud(params, 3, rest))
+        scene_views.append([(v.camera(), im) for v, im in zip(views, images)])
+    cfg = TrainConfig(iterations=100, sh_degree=3, sh_increase_interval=0,
+                      densify_from_iteration=1000, densify_until_iteration=1000)
+    joint = px.SplatTrainer.from_scenes(clouds, scene_views, cfg)
+    single = [px.SplatTrainer(c, sv, cfg) for c, sv in zip(clouds, scene_views)]
+    for step in range(3):
+        ids = [s * 3 + (step + k) % 3 for s in range(3) for k in range(2)]  # 2 views a scene
+        loss = joint.step_batch(len(ids), ids)
+        losses = [t.step_batch(2, [(step + k) % 3 for k in range(2)]) for t in single]
+        assert abs(loss - float(np.mean(losses))) <= 1e-5 * abs(loss)
+    joined = joint.cloud_params()
+    at = 0
+    for c, t in zip(clouds, single):
+        mine = joined[:, at:at + c.count]
+        at += c.count
+        assert np.abs(mine - t.cloud_params()).max() <= 1e-4
+    # one scene of the joint trainer trains apart from the others
+    with pytest.raises(px.PxsError):
+        joint.finish()
+    bad = TrainConfig(iterations=100, densify_from_iteration=10, densify_until_iteration=50)
+    with pytest.raises(px.PxsError):
+        px.SplatTrainer.from_scenes(clouds, scene_views, bad)
+    for t in single + [joint]:
+        t.close()
