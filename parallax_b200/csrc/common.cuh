@@ -37,7 +37,7 @@ struct ViewDesc {
   float min_alpha;
   float transmittance_cutoff;
   float screen_dilation;
-  int32_t pad1;
+  int32_t loss_tile_offset;  // first 32x16 tile of this view in the loss kernel's flat grid
   int64_t target_offset;     // first pixel of this view's target image
   // the gaussians this view renders: [gauss_offset, gauss_offset + gauss_count)
   // of the parameter arrays; slot v * slot_stride + i holds gaussian

@@ -119,9 +119,15 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
 // loss.cu
 size_t loss_smem_bytes();
 void configure_loss_kernel();  // once per device, outside graph capture
+// Output tiles of one view in the loss kernel.
+int64_t loss_tiles(int width, int height);
+// `flat_tiles` >= 0: a one-dimensional grid of that many CTAs over every
+// view's own tiles (the sum of loss_tiles over the views); otherwise a grid
+// sized for the largest view.
 void launch_loss(const float* rendered, const float* target, const ViewDesc* views, int n_views,
                  int max_width, int max_height, const LossParams& lp, float* grad_out,
-                 double* sums, float* per_view, float* total, cudaStream_t stream);
+                 double* sums, float* per_view, float* total, cudaStream_t stream,
+                 int64_t flat_tiles = -1);
 
 // peak.cu
 float measure_fp32_peak_tflops(cudaStream_t stream);

@@ -37,16 +37,34 @@ struct LossSmem {
 }  // namespace
 
 // mode 0: dL/drgb of photometricLoss; mode 1: d(mean SSIM)/drgb (meanSsim).
+// With `flat`, the grid is one-dimensional over every view's own output tiles,
+// view after view (views of different sizes waste no CTAs); otherwise the
+// grid is (tiles across, tiles down, view) for the largest view.
 __global__ void __launch_bounds__(kThreads)
     k_loss(const float* __restrict__ rendered, const float* __restrict__ target,
            const ViewDesc* __restrict__ views, int n_views, LossParams lp,
-           float* __restrict__ grad_out, double* __restrict__ sums) {
+           float* __restrict__ grad_out, double* __restrict__ sums, int flat) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LossSmem& sm = *reinterpret_cast<LossSmem*>(smem_raw);
-  const int v = blockIdx.z;
+  int v = blockIdx.z, ox = blockIdx.x * TW, oy = blockIdx.y * TH;
+  if (flat) {
+    // the last view whose first tile is at or before this CTA's
+    const int t = blockIdx.x;
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (views[mid].loss_tile_offset <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    v = lo;
+    const int local = t - views[v].loss_tile_offset;
+    const int across = (views[v].cam.width + TW - 1) / TW;
+    if (across == 0) return;
+    ox = (local % across) * TW;
+    oy = (local / across) * TH;
+  }
   const ViewDesc& vd = views[v];
   const int W = vd.cam.width, H = vd.cam.height;
-  const int ox = blockIdx.x * TW, oy = blockIdx.y * TH;
   if (ox >= W || oy >= H) return;
   const int64_t pix0 = vd.pixel_offset;
   const float* rimg = rendered + pix0 * 3;
@@ -295,15 +313,26 @@ void configure_loss_kernel() {
                        (int)sizeof(LossSmem));
 }
 
+int64_t loss_tiles(int width, int height) {
+  return (int64_t)((width + TW - 1) / TW) * ((height + TH - 1) / TH);
+}
+
 void launch_loss(const float* rendered, const float* target, const ViewDesc* views, int n_views,
                  int max_width, int max_height, const LossParams& lp, float* grad_out,
-                 double* sums, float* per_view, float* total, cudaStream_t stream) {
+                 double* sums, float* per_view, float* total, cudaStream_t stream,
+                 int64_t flat_tiles) {
   if (n_views <= 0) return;
   cudaMemsetAsync(sums, 0, sizeof(double) * 2 * n_views, stream);
-  dim3 grid((max_width + TW - 1) / TW, (max_height + TH - 1) / TH, n_views);
   count_launch();
-  k_loss<<<grid, kThreads, sizeof(LossSmem), stream>>>(rendered, target, views, n_views, lp,
-                                                       grad_out, sums);
+  if (flat_tiles >= 0) {
+    if (flat_tiles > 0)
+      k_loss<<<(unsigned)flat_tiles, kThreads, sizeof(LossSmem), stream>>>(
+          rendered, target, views, n_views, lp, grad_out, sums, 1);
+  } else {
+    dim3 grid((max_width + TW - 1) / TW, (max_height + TH - 1) / TH, n_views);
+    k_loss<<<grid, kThreads, sizeof(LossSmem), stream>>>(rendered, target, views, n_views, lp,
+                                                         grad_out, sums, 0);
+  }
   count_launch();
   k_loss_finalize<<<1, 32, 0, stream>>>(sums, views, n_views, lp.ssim_weight, lp.mode,
                                         per_view, total);

@@ -39,6 +39,7 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
   ViewBatch b;
   b.views.resize(static_cast<size_t>(n_views));
   int tile_offset = 0, row_offset = 0;
+  int64_t loss_tile_offset = 0;
   int64_t pixel_offset = 0;
   for (int v = 0; v < n_views; ++v) {
     ViewDesc& d = b.views[static_cast<size_t>(v)];
@@ -53,6 +54,8 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
       throw Error(PXS_ERR_INVALID, "image too large (at most 2048 tiles across)");
     d.tile_offset = tile_offset;
     d.row_offset = row_offset;
+    d.loss_tile_offset = static_cast<int32_t>(loss_tile_offset);
+    loss_tile_offset += loss_tiles(d.cam.width, d.cam.height);
     d.pixel_offset = pixel_offset;
     d.target_offset = pixel_offset;
     d.min_alpha = options.min_alpha;
@@ -287,8 +290,10 @@ void Frame::loss(const float* target, float ssim_weight, int mode, float* grad_o
   ssim_kernel_weights(lp.kernel);
   lp.ssim_weight = ssim_weight;
   lp.mode = mode;
+  int64_t tiles = 0;
+  for (const ViewDesc& d : batch.views) tiles += loss_tiles(d.cam.width, d.cam.height);
   launch_loss(rgb.get(), target, d_views.get(), V, batch.max_width, batch.max_height, lp,
-              grad_out, loss_sums.get(), loss_per_view.get(), loss_total.get(), stream);
+              grad_out, loss_sums.get(), loss_per_view.get(), loss_total.get(), stream, tiles);
   PXS_CUDA(cudaGetLastError());
 }
 
