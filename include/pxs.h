@@ -447,6 +447,27 @@ int pxs_densify_and_prune(pxs_context* context, float* params, int32_t* count,
                           int32_t* source_index, int32_t* cloned, int32_t* split,
                           int32_t* pruned);
 
+/* ------------------------------------------------------- trained-cloud files
+ * The reference's writers (GaussianCloud.h:95-131) into memory: the bytes of
+ * the file writeGaussianPly (GaussianCloud.cpp:259-306), writeSplat
+ * (:414-443) or writeSpz (:493-550; `fractional_bits` clamped to 0..20 as
+ * there) would write for the cloud. The body is packed on the device
+ * (transposed and quantised) and copied back once; .spz is then gzipped on the
+ * host with the reference's deflate settings. `out` receives at most
+ * `capacity` bytes and `size` the file's size; with `out` NULL or too small
+ * the call returns PXS_ERR_CAPACITY and only sets `size`. An empty cloud is
+ * PXS_ERR_INVALID (the reference returns false), as is .spz above SH
+ * degree 3. */
+#define PXS_FORMAT_PLY 0
+#define PXS_FORMAT_SPLAT 1
+#define PXS_FORMAT_SPZ 2
+int pxs_export_cloud(pxs_context* context, const pxs_cloud* cloud, int32_t format,
+                     int32_t fractional_bits, uint8_t* out, size_t capacity, size_t* size);
+/* The same for a trainer's current cloud, already on the device (a trainer
+ * over several scenes is refused: download and split it instead). */
+int pxs_trainer_export(pxs_trainer* trainer, int32_t format, int32_t fractional_bits,
+                       uint8_t* out, size_t capacity, size_t* size);
+
 /* -------------------------------------------------------- synthetic scenes
  * Seeded generators for the benchmark workloads. The generator is the
  * reference's xorshift64 Rng with a Box-Muller normal

@@ -397,6 +397,16 @@ int ref_trainer_finish(void* handle, float* params, int capacity, int* sh_degree
   return fromCloud(cloud, h->rest, params, capacity);
 }
 
+// writeGaussianPly / writeSplat / writeSpz (GaussianCloud.cpp:259-306, 414-443,
+// 493-550) of the cloud into `path`; format 0, 1, 2. Returns the writer's result.
+int ref_write_cloud(const float* params, int n, int rest, int cloud_sh, int format,
+                    int fractional_bits, const char* path) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  if (format == 0) return writeGaussianPly(path, cloud) ? 1 : 0;
+  if (format == 1) return writeSplat(path, cloud) ? 1 : 0;
+  return writeSpz(path, cloud, fractional_bits) ? 1 : 0;
+}
+
 int ref_config_validate(const pxs_train_config* config, char* reason, int len) {
   const std::string why = toConfig(config).validate();
   if (reason != nullptr && len > 0) {

@@ -24,6 +24,7 @@ from .splat import (  # noqa: F401
     SplatView,
     default_context,
     densify_and_prune,
+    export_cloud,
     mean_ssim,
     photometric_loss,
     project_splats,

@@ -17,6 +17,10 @@ PXS_ERR_CAPACITY = 4
 PXS_ERR_UNAVAILABLE = 5
 PXS_ERR_TIMEOUT = 6
 
+PXS_FORMAT_PLY = 0
+PXS_FORMAT_SPLAT = 1
+PXS_FORMAT_SPZ = 2
+
 TILE = 16
 C_POSITION, C_LOG_SCALE, C_ROTATION, C_OPACITY, C_DC, C_SH_REST = 0, 3, 6, 10, 11, 14
 

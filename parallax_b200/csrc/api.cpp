@@ -27,6 +27,8 @@ struct pxs_context {
   DeviceArray<float> acc_gradient, out_params;
   DeviceArray<int32_t> acc_views, source;
   pxs::DensifyWork densify;
+  DeviceArray<uint8_t> export_body;
+  DeviceArray<int32_t> export_fields;
 };
 
 namespace {
@@ -549,6 +551,34 @@ int pxs_adam_device(pxs_context* ctx, float* params, float* grads, float* m, flo
     PXS_CUDA(cudaGetLastError());
     PXS_CUDA(cudaStreamSynchronize(ctx->stream));
   });
+}
+
+// Copies `bytes` out, or reports the size needed.
+static int deliver_bytes(const std::vector<uint8_t>& bytes, uint8_t* out, size_t capacity,
+                         size_t* size) {
+  if (size != nullptr) *size = bytes.size();
+  if (out == nullptr || capacity < bytes.size()) return PXS_ERR_CAPACITY;
+  std::memcpy(out, bytes.data(), bytes.size());
+  return PXS_OK;
+}
+
+int pxs_export_cloud(pxs_context* ctx, const pxs_cloud* cloud, int32_t format,
+                     int32_t fractional_bits, uint8_t* out, size_t capacity, size_t* size) {
+  std::vector<uint8_t> bytes;
+  const int status = guarded(ctx, [&] {
+    validate_cloud(cloud);
+    if (cloud->count <= 0) throw Error(PXS_ERR_INVALID, "the cloud is empty");
+    const size_t values =
+        static_cast<size_t>(PXS_PARAM_COUNT(cloud->rest_per_channel)) * cloud->count;
+    float* d = ctx->params.reserve(values);
+    PXS_CUDA(cudaMemcpyAsync(d, cloud->params, values * sizeof(float), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    bytes = pxs::export_cloud_bytes(d, cloud->count, cloud->rest_per_channel, cloud->sh_degree,
+                                    format, fractional_bits, ctx->export_body,
+                                    ctx->export_fields, ctx->stream);
+  });
+  if (status != PXS_OK) return status;
+  return deliver_bytes(bytes, out, capacity, size);
 }
 
 int pxs_densify_and_prune(pxs_context* ctx, float* params, int32_t* count,

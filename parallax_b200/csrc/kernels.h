@@ -129,6 +129,13 @@ void launch_loss(const float* rendered, const float* target, const ViewDesc* vie
                  double* sums, float* per_view, float* total, cudaStream_t stream,
                  int64_t flat_tiles = -1);
 
+// export.cu: the reference's file formats packed on the device
+void launch_pack_ply(const float* params, int n, const int* field_src, int fields, float* out,
+                     cudaStream_t stream);
+void launch_pack_splat(const float* params, int n, uint8_t* out, cudaStream_t stream);
+void launch_pack_spz(const float* params, int n, int fractional_bits, int rest_stored,
+                     int rest_degree, uint8_t* out, cudaStream_t stream);
+
 // peak.cu
 float measure_fp32_peak_tflops(cudaStream_t stream);
 

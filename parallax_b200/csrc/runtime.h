@@ -99,6 +99,13 @@ struct ViewBatch {
   bool own_ranges = false;
 };
 
+// The bytes of a cloud's file in `format` (PXS_FORMAT_*), packed on the device
+// from component-major device params and copied back once.
+std::vector<uint8_t> export_cloud_bytes(const float* d_params, int n, int S, int sh_degree,
+                                        int format, int fractional_bits,
+                                        DeviceArray<uint8_t>& body, DeviceArray<int32_t>& fields,
+                                        cudaStream_t stream);
+
 ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_options& options,
                      int cloud_sh_degree);
 int bits_for(int64_t count);  // bits to represent values in [0, count)

@@ -932,6 +932,24 @@ int pxs_trainer_finish(pxs_trainer* t, float* params, int32_t capacity, int32_t*
   });
 }
 
+int pxs_trainer_export(pxs_trainer* t, int32_t format, int32_t fractional_bits, uint8_t* out,
+                       size_t capacity, size_t* size) {
+  std::vector<uint8_t> bytes;
+  const int status = guarded(t, [&] {
+    if (t->n_scenes > 1)
+      throw Error(PXS_ERR_INVALID, "a trainer over several scenes exports no single file");
+    DeviceArray<uint8_t> body;
+    DeviceArray<int32_t> fields;
+    bytes = pxs::export_cloud_bytes(t->params.get(), t->N, t->S, t->cloud_sh, format,
+                                    fractional_bits, body, fields, t->stream);
+  });
+  if (status != PXS_OK) return status;
+  if (size != nullptr) *size = bytes.size();
+  if (out == nullptr || capacity < bytes.size()) return PXS_ERR_CAPACITY;
+  std::memcpy(out, bytes.data(), bytes.size());
+  return PXS_OK;
+}
+
 int pxs_trainer_create_scenes(const pxs_train_config* config, const pxs_cloud* clouds,
                               int32_t n_scenes, const int32_t* views_per_scene,
                               const pxs_camera* cameras, const float* const* images,

@@ -399,6 +399,13 @@ class SplatTrainer:
         return [(g.value, P.value * n.value, "float32"), (sg.value, n.value, "float32"),
                 (vc.value, n.value, "int32")]
 
+    def export(self, fmt: str = "ply", fractional_bits: int = 12) -> bytes:
+        """The trained cloud as the bytes of a .ply, .splat or .spz file."""
+        status, data = _export(lambda out, cap, size: self._lib.pxs_trainer_export(
+            self.handle, FORMATS[fmt], fractional_bits, out, cap, size), fmt)
+        self._check(status)
+        return data
+
     def stream(self) -> int:
         """The trainer's CUDA stream (a cudaStream_t as an integer)."""
         sp = ct.c_void_p()
@@ -466,6 +473,31 @@ class SplatTrainer:
             self.close()
         except Exception:
             pass
+
+
+FORMATS = {"ply": A.PXS_FORMAT_PLY, "splat": A.PXS_FORMAT_SPLAT, "spz": A.PXS_FORMAT_SPZ}
+
+
+def _export(call, fmt: str) -> bytes:
+    size = ct.c_size_t()
+    status = call(None, 0, ct.byref(size))
+    if status not in (A.PXS_OK, A.PXS_ERR_CAPACITY):
+        return status, b""
+    buf = (ct.c_uint8 * max(size.value, 1))()
+    status = call(buf, size.value, ct.byref(size))
+    return status, bytes(buf[: size.value])
+
+
+def export_cloud(cloud: GaussianCloud, fmt: str = "ply", fractional_bits: int = 12,
+                 ctx: Optional[Context] = None) -> bytes:
+    """The bytes writeGaussianPly / writeSplat / writeSpz (GaussianCloud.h:95-131)
+    would write for `cloud`, packed on the device: fmt is "ply", "splat" or "spz"."""
+    ctx = ctx or default_context()
+    c = cloud.c_struct()
+    status, data = _export(lambda out, cap, size: lib().pxs_export_cloud(
+        ctx.handle, ct.byref(c), FORMATS[fmt], fractional_bits, out, cap, size), fmt)
+    ctx.check(status)
+    return data
 
 
 def train_splats_on_gpu(cloud: GaussianCloud, views, config: A.TrainConfig,

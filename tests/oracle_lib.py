@@ -109,6 +109,20 @@ def ref(kind: str = "ieee") -> ct.CDLL:
     return _REF[kind]
 
 
+_LIBM = ct.CDLL("libm.so.6")
+_LIBM.expf.restype = ct.c_float
+_LIBM.expf.argtypes = [ct.c_float]
+
+
+def glibc_exp_is_correctly_rounded(values):
+    """Per value: does glibc's expf (the oracle's and the reference's) equal the
+    correctly rounded exp the device computes?"""
+    flat = np.asarray(values, dtype=np.float32).reshape(-1)
+    cr = np.exp(flat.astype(np.float64)).astype(np.float32)
+    glibc = np.array([_LIBM.expf(float(x)) for x in flat], dtype=np.float32)
+    return (cr.view(np.uint32) == glibc.view(np.uint32)).reshape(np.shape(values))
+
+
 # ---------------------------------------------------------------- scenes
 
 

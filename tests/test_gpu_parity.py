@@ -88,18 +88,7 @@ def make_case(case):
     return random_case(40 + sh, 3000, sh, 200 + 8 * sh, 150 - 5 * sh)
 
 
-_LIBM = ct.CDLL("libm.so.6")
-_LIBM.expf.restype = ct.c_float
-_LIBM.expf.argtypes = [ct.c_float]
-
-
-def glibc_exp_is_correctly_rounded(values):
-    """Per value: does glibc's expf (the oracle's and the reference's) equal the
-    correctly rounded exp the device computes?"""
-    flat = np.asarray(values, dtype=np.float32).reshape(-1)
-    cr = np.exp(flat.astype(np.float64)).astype(np.float32)
-    glibc = np.array([_LIBM.expf(float(x)) for x in flat], dtype=np.float32)
-    return (cr.view(np.uint32) == glibc.view(np.uint32)).reshape(np.shape(values))
+glibc_exp_is_correctly_rounded = O.glibc_exp_is_correctly_rounded
 
 
 @pytest.mark.parametrize("case", CASES)
