@@ -447,6 +447,23 @@ int pxs_densify_and_prune(pxs_context* context, float* params, int32_t* count,
                           int32_t* source_index, int32_t* cloned, int32_t* split,
                           int32_t* pruned);
 
+/* ---------------------------------------------------------- image ingest
+ * The training images of Pipeline::Impl::runSplatTraining
+ * (Pipeline.cpp:1892-1917): an 8-bit RGB frame box-filtered to a target width
+ * by downscaleToWidth (ImageIo.cpp:300-337, the frame unchanged when it is no
+ * wider), each byte then divided by 255. pxs_downscale_to_width runs it on the
+ * device for host buffers: out_rgb gets the downscaled bytes and out_linear
+ * the floats (either may be NULL; with both NULL only the size is written).
+ * pxs_trainer_ingest_images replaces the resident images of `view_ids` from
+ * 8-bit frames, downscaled to each view's width on the device (the result
+ * must have the view's size); only the 8-bit frames cross to the device. */
+int pxs_downscale_to_width(pxs_context* context, const uint8_t* rgb, int32_t width,
+                           int32_t height, int32_t target_width, uint8_t* out_rgb,
+                           float* out_linear, int32_t* out_width, int32_t* out_height);
+int pxs_trainer_ingest_images(pxs_trainer* trainer, int32_t n, const int32_t* view_ids,
+                              const uint8_t* const* frames, const int32_t* widths,
+                              const int32_t* heights);
+
 /* ------------------------------------------------------- trained-cloud files
  * The reference's writers (GaussianCloud.h:95-131) into memory: the bytes of
  * the file writeGaussianPly (GaussianCloud.cpp:259-306), writeSplat

@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "parallax/io/ImageIo.h"
 #include "parallax/splat/SplatDensify.h"
 #include "parallax/splat/SplatRaster.h"
 #include "parallax/splat/SplatTrainer.h"
@@ -405,6 +406,18 @@ int ref_write_cloud(const float* params, int n, int rest, int cloud_sh, int form
   if (format == 0) return writeGaussianPly(path, cloud) ? 1 : 0;
   if (format == 1) return writeSplat(path, cloud) ? 1 : 0;
   return writeSpz(path, cloud, fractional_bits) ? 1 : 0;
+}
+
+// downscaleToWidth (ImageIo.cpp:300-337); returns the output width and height
+// through w / h and writes the bytes when `out` is given.
+void ref_downscale(const uint8_t* rgb, int width, int height, int target_width, uint8_t* out,
+                   int* w, int* h) {
+  ColorBuffer image(width, height);
+  std::memcpy(image.pixels.data(), rgb, static_cast<size_t>(width) * height * 3);
+  const ColorBuffer scaled = downscaleToWidth(image, target_width);
+  *w = scaled.width;
+  *h = scaled.height;
+  if (out != nullptr) std::memcpy(out, scaled.pixels.data(), scaled.pixels.size());
 }
 
 int ref_config_validate(const pxs_train_config* config, char* reason, int len) {

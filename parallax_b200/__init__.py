@@ -24,6 +24,7 @@ from .splat import (  # noqa: F401
     SplatView,
     default_context,
     densify_and_prune,
+    downscale_to_width,
     export_cloud,
     mean_ssim,
     photometric_loss,

@@ -29,6 +29,7 @@ struct pxs_context {
   pxs::DensifyWork densify;
   DeviceArray<uint8_t> export_body;
   DeviceArray<int32_t> export_fields;
+  DeviceArray<uint8_t> ingest_in, ingest_bytes;
 };
 
 namespace {
@@ -549,6 +550,34 @@ int pxs_adam_device(pxs_context* ctx, float* params, float* grads, float* m, flo
     pxs::launch_adam(params, grads, m, v, count, rest_per_channel, d, zero_grads, nullptr,
                      nullptr, nullptr, nullptr, ctx->stream);
     PXS_CUDA(cudaGetLastError());
+    PXS_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int pxs_downscale_to_width(pxs_context* ctx, const uint8_t* rgb, int32_t width, int32_t height,
+                           int32_t target_width, uint8_t* out_rgb, float* out_linear,
+                           int32_t* out_width, int32_t* out_height) {
+  return guarded(ctx, [&] {
+    if (width < 0 || height < 0) throw Error(PXS_ERR_INVALID, "negative image size");
+    int w = 0, h = 0;
+    pxs::downscaled_size(width, height, target_width, &w, &h);
+    if (out_width) *out_width = w;
+    if (out_height) *out_height = h;
+    const size_t in_bytes = static_cast<size_t>(width) * height * 3;
+    const size_t out_values = static_cast<size_t>(w) * h * 3;
+    if ((out_rgb == nullptr && out_linear == nullptr) || out_values == 0) return;
+    if (rgb == nullptr) throw Error(PXS_ERR_INVALID, "image is null");
+    uint8_t* d_in = ctx->ingest_in.reserve(in_bytes);
+    PXS_CUDA(cudaMemcpyAsync(d_in, rgb, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    uint8_t* d_bytes = out_rgb ? ctx->ingest_bytes.reserve(out_values) : nullptr;
+    float* d_lin = out_linear ? ctx->image_a.reserve(out_values) : nullptr;
+    pxs::launch_downscale(d_in, width, height, w, h, d_bytes, d_lin, ctx->stream);
+    PXS_CUDA(cudaGetLastError());
+    if (out_rgb)
+      PXS_CUDA(cudaMemcpyAsync(out_rgb, d_bytes, out_values, cudaMemcpyDeviceToHost, ctx->stream));
+    if (out_linear)
+      PXS_CUDA(cudaMemcpyAsync(out_linear, d_lin, out_values * sizeof(float),
+                               cudaMemcpyDeviceToHost, ctx->stream));
     PXS_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }

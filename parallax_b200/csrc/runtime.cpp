@@ -34,6 +34,17 @@ void ssim_kernel_weights(float out[11]) {
   for (int i = 0; i < 11; ++i) out[i] /= total;
 }
 
+void downscaled_size(int width, int height, int target_width, int* out_width, int* out_height) {
+  if (width <= 0 || height <= 0 || target_width <= 0 || width <= target_width) {
+    *out_width = width;
+    *out_height = height;
+    return;
+  }
+  *out_width = target_width;
+  *out_height = std::max(1, static_cast<int>(std::lround(static_cast<double>(height) *
+                                                          target_width / width)));
+}
+
 ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_options& options,
                      int cloud_sh_degree) {
   ViewBatch b;

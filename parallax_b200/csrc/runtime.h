@@ -106,6 +106,10 @@ std::vector<uint8_t> export_cloud_bytes(const float* d_params, int n, int S, int
                                         DeviceArray<uint8_t>& body, DeviceArray<int32_t>& fields,
                                         cudaStream_t stream);
 
+// downscaleToWidth's output size (ImageIo.cpp:300-304): the image itself when
+// it is no wider than the target.
+void downscaled_size(int width, int height, int target_width, int* out_width, int* out_height);
+
 ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_options& options,
                      int cloud_sh_degree);
 int bits_for(int64_t count);  // bits to represent values in [0, count)

@@ -65,6 +65,7 @@ struct pxs_trainer {
   std::vector<pxs_camera> cameras;
   std::vector<int64_t> image_offset;  // first pixel of each view in `images`
   DeviceArray<float> images;
+  DeviceArray<uint8_t> ingest_in;  // staging for 8-bit frames
 
   int iteration = 0;
   float extent = 1.f, last_loss = 0.f, smoothed_loss = 0.f;
@@ -929,6 +930,37 @@ int pxs_trainer_finish(pxs_trainer* t, float* params, int32_t capacity, int32_t*
     t->N = static_cast<int>(n);
     t->cloud_sh = t->cfg.sh_degree;
     t->iteration = t->cfg.iterations;
+  });
+}
+
+int pxs_trainer_ingest_images(pxs_trainer* t, int32_t n, const int32_t* view_ids,
+                              const uint8_t* const* frames, const int32_t* widths,
+                              const int32_t* heights) {
+  return guarded(t, [&] {
+    if (n < 0 || (n > 0 && (view_ids == nullptr || frames == nullptr || widths == nullptr ||
+                            heights == nullptr)))
+      throw Error(PXS_ERR_INVALID, "null argument");
+    for (int i = 0; i < n; ++i) {
+      const int id = view_ids[i];
+      if (id < 0 || id >= static_cast<int>(t->cameras.size()))
+        throw Error(PXS_ERR_INVALID, "view id out of range");
+      const pxs_camera& cam = t->cameras[static_cast<size_t>(id)];
+      int w = 0, h = 0;
+      pxs::downscaled_size(widths[i], heights[i], cam.width, &w, &h);
+      if (w != cam.width || h != cam.height)
+        throw Error(PXS_ERR_INVALID, "the downscaled frame does not match the view's size");
+      const size_t in_bytes = static_cast<size_t>(widths[i]) * heights[i] * 3;
+      if (in_bytes == 0) continue;
+      if (frames[i] == nullptr) throw Error(PXS_ERR_INVALID, "frame is null");
+      uint8_t* d_in = t->ingest_in.reserve(in_bytes);
+      PXS_CUDA(cudaMemcpyAsync(d_in, frames[i], in_bytes, cudaMemcpyHostToDevice, t->stream));
+      pxs::launch_downscale(d_in, widths[i], heights[i], w, h, nullptr,
+                            t->images.get() + t->image_offset[static_cast<size_t>(id)] * 3,
+                            t->stream);
+      PXS_CUDA(cudaGetLastError());
+      // the staging buffer is reused by the next frame: wait for this one
+      PXS_CUDA(cudaStreamSynchronize(t->stream));
+    }
   });
 }
 

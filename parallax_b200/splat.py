@@ -399,6 +399,18 @@ class SplatTrainer:
         return [(g.value, P.value * n.value, "float32"), (sg.value, n.value, "float32"),
                 (vc.value, n.value, "int32")]
 
+    def ingest_images(self, view_ids: Sequence[int], frames: Sequence[np.ndarray],
+                      sizes: Sequence[Tuple[int, int]]) -> None:
+        """Replaces the resident images of `view_ids` from 8-bit RGB frames of
+        the given (width, height), downscaled on the device to each view's size."""
+        n = len(view_ids)
+        keep = [np.ascontiguousarray(f, dtype=np.uint8) for f in frames]
+        ids = (ct.c_int32 * max(n, 1))(*view_ids)
+        ptrs = (ct.c_void_p * max(n, 1))(*[f.ctypes.data for f in keep])
+        ws = (ct.c_int32 * max(n, 1))(*[s[0] for s in sizes])
+        hs = (ct.c_int32 * max(n, 1))(*[s[1] for s in sizes])
+        self._check(self._lib.pxs_trainer_ingest_images(self.handle, n, ids, ptrs, ws, hs))
+
     def export(self, fmt: str = "ply", fractional_bits: int = 12) -> bytes:
         """The trained cloud as the bytes of a .ply, .splat or .spz file."""
         status, data = _export(lambda out, cap, size: self._lib.pxs_trainer_export(
@@ -498,6 +510,23 @@ def export_cloud(cloud: GaussianCloud, fmt: str = "ply", fractional_bits: int = 
         ctx.handle, ct.byref(c), FORMATS[fmt], fractional_bits, out, cap, size), fmt)
     ctx.check(status)
     return data
+
+
+def downscale_to_width(rgb: np.ndarray, width: int, height: int, target_width: int,
+                       ctx: Optional[Context] = None):
+    """downscaleToWidth (ImageIo.cpp:300-337) on the device: (bytes H*W*3 uint8,
+    floats H*W*3 = bytes / 255, out_width, out_height)."""
+    ctx = ctx or default_context()
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    w, h = ct.c_int32(), ct.c_int32()
+    ctx.check(lib().pxs_downscale_to_width(ctx.handle, None, width, height, target_width, None,
+                                           None, ct.byref(w), ct.byref(h)))
+    out = np.zeros(w.value * h.value * 3, dtype=np.uint8)
+    lin = np.zeros(w.value * h.value * 3, dtype=np.float32)
+    ctx.check(lib().pxs_downscale_to_width(ctx.handle, rgb.ctypes.data, width, height,
+                                           target_width, out.ctypes.data, lin.ctypes.data,
+                                           ct.byref(w), ct.byref(h)))
+    return out, lin, w.value, h.value
 
 
 def train_splats_on_gpu(cloud: GaussianCloud, views, config: A.TrainConfig,

@@ -1,0 +1,62 @@
+"""Image ingest: downscaleToWidth (ImageIo.cpp:300-337) and the /255 to the
+float training image (Pipeline.cpp:1904-1913), run on the device, against the
+reference's own function. Integer arithmetic: bit-exact."""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import parallax_b200 as px
+
+
+def reference_downscale(rgb, width, height, target):
+    lib = O.ref()
+    lib.ref_downscale.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p,
+                                  ct.c_void_p, ct.c_void_p]
+    w, h = ct.c_int(), ct.c_int()
+    lib.ref_downscale(rgb.ctypes.data, width, height, target, None, ct.byref(w), ct.byref(h))
+    out = np.zeros(w.value * h.value * 3, np.uint8)
+    lib.ref_downscale(rgb.ctypes.data, width, height, target, out.ctypes.data, ct.byref(w),
+                      ct.byref(h))
+    return out, w.value, h.value
+
+
+CASES = [(1920, 1080, 640), (1279, 719, 320), (640, 480, 640), (300, 200, 400), (7, 5, 3),
+         (4032, 3024, 1280), (1, 1, 1), (513, 1, 100)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width,height,target", CASES)
+def test_downscale_matches_the_reference(width, height, target):
+    rgb = np.random.default_rng(width * 31 + height).integers(0, 256, width * height * 3,
+                                                               dtype=np.uint8)
+    ref, rw, rh = reference_downscale(rgb, width, height, target)
+    out, lin, w, h = px.downscale_to_width(rgb, width, height, target)
+    assert (w, h) == (rw, rh)
+    assert np.array_equal(out, ref)
+    assert np.array_equal(lin, ref.astype(np.float32) / np.float32(255.0))
+
+
+@pytest.mark.gpu
+def test_trainer_ingests_frames_at_its_view_size():
+    params, rest = O.random_cloud(71, 500, 0)
+    cloud = px.GaussianCloud(params, 0, rest)
+    frames = [np.random.default_rng(k).integers(0, 256, 1280 * 720 * 3, dtype=np.uint8)
+              for k in range(2)]
+    expect = [reference_downscale(f, 1280, 720, 320) for f in frames]
+    views = O.orbit_views(2, 320, 180, seed=3)
+    t = px.SplatTrainer(cloud, [(v.camera(), np.zeros(320 * 180 * 3, np.float32))
+                                for v in views], px.TrainConfig(iterations=2))
+    t.ingest_images([0, 1], frames, [(1280, 720)] * 2)
+    # the resident images are the floats: render-and-score through them is
+    # the same as with the host-converted images
+    a = px.SplatTrainer(cloud, [(v.camera(), e[0].astype(np.float32) / np.float32(255.0))
+                                for v, e in zip(views, expect)], px.TrainConfig(iterations=2))
+    assert t.step_batch(2, [0, 1]) == a.step_batch(2, [0, 1])
+    with pytest.raises(px.PxsError):  # a 1280x800 frame at width 320 is 320x200, not 320x180
+        t.ingest_images([0], [np.zeros(1280 * 800 * 3, np.uint8)], [(1280, 800)])
+    for x in (t, a):
+        x.close()
