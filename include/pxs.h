@@ -447,6 +447,19 @@ int pxs_densify_and_prune(pxs_context* context, float* params, int32_t* count,
                           int32_t* source_index, int32_t* cloned, int32_t* split,
                           int32_t* pruned);
 
+/* initializeFromPointCloud (GaussianCloud.cpp:199-257), the pipeline's seed
+ * for training: one isotropic gaussian per point (n points, x y z floats),
+ * sigma half the mean nearest-neighbour distance over a sample of at most 512
+ * points (searched on the device), identity rotation, opacity logit from
+ * `initial_opacity`, DC from the point's 8-bit colour (`colors` may be NULL),
+ * zero higher SH. sh_degree is clamped to 0..3; `rest_per_channel` receives
+ * its SH-rest count and `params` (may be NULL to ask only for that) receives
+ * the component-major cloud, 14 + 3 * rest_per_channel rows of n. */
+int pxs_initialize_from_points(pxs_context* context, const float* points,
+                               const uint8_t* colors, int32_t n, int32_t sh_degree,
+                               float initial_opacity, float* params,
+                               int32_t* rest_per_channel);
+
 /* ---------------------------------------------------------- image ingest
  * The training images of Pipeline::Impl::runSplatTraining
  * (Pipeline.cpp:1892-1917): an 8-bit RGB frame box-filtered to a target width

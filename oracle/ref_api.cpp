@@ -420,6 +420,21 @@ void ref_downscale(const uint8_t* rgb, int width, int height, int target_width, 
   if (out != nullptr) std::memcpy(out, scaled.pixels.data(), scaled.pixels.size());
 }
 
+// initializeFromPointCloud (GaussianCloud.cpp:199-257) into `params`
+// (component-major); returns the gaussian count.
+int ref_initialize_from_points(const float* points, const uint8_t* colors, int n, int sh_degree,
+                               float initial_opacity, float* params) {
+  std::vector<Vec3f> pts(static_cast<size_t>(n));
+  std::vector<std::array<uint8_t, 3>> cols;
+  for (int i = 0; i < n; ++i) {
+    pts[static_cast<size_t>(i)] = Vec3f(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    if (colors != nullptr) cols.push_back({colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]});
+  }
+  const GaussianCloud cloud = initializeFromPointCloud(pts, cols, sh_degree, initial_opacity);
+  const int rest = shRestPerChannel(cloud.sh_degree);
+  return fromCloud(cloud, rest, params, n);
+}
+
 int ref_config_validate(const pxs_train_config* config, char* reason, int len) {
   const std::string why = toConfig(config).validate();
   if (reason != nullptr && len > 0) {

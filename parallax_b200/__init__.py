@@ -26,6 +26,7 @@ from .splat import (  # noqa: F401
     densify_and_prune,
     downscale_to_width,
     export_cloud,
+    initialize_from_points,
     mean_ssim,
     photometric_loss,
     project_splats,

@@ -76,6 +76,7 @@ def _declare(lib: ct.CDLL) -> None:
         "pxs_trainer_create_scenes": (ct.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _i32, _vp]),
         "pxs_export_cloud": (ct.c_int, [_vp, _vp, _i32, _i32, _vp, ct.c_size_t, _vp]),
         "pxs_downscale_to_width": (ct.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
+        "pxs_initialize_from_points": (ct.c_int, [_vp, _vp, _vp, _i32, _i32, _f32, _vp, _vp]),
         "pxs_trainer_ingest_images": (ct.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
         "pxs_trainer_export": (ct.c_int, [_vp, _i32, _i32, _vp, ct.c_size_t, _vp]),
         "pxs_trainer_apply": (ct.c_int, [_vp, _f32]),

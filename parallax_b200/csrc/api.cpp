@@ -30,6 +30,7 @@ struct pxs_context {
   DeviceArray<uint8_t> export_body;
   DeviceArray<int32_t> export_fields;
   DeviceArray<uint8_t> ingest_in, ingest_bytes;
+  DeviceArray<double> seed_nearest;
 };
 
 namespace {
@@ -550,6 +551,60 @@ int pxs_adam_device(pxs_context* ctx, float* params, float* grads, float* m, flo
     pxs::launch_adam(params, grads, m, v, count, rest_per_channel, d, zero_grads, nullptr,
                      nullptr, nullptr, nullptr, ctx->stream);
     PXS_CUDA(cudaGetLastError());
+    PXS_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int pxs_initialize_from_points(pxs_context* ctx, const float* points, const uint8_t* colors,
+                               int32_t n, int32_t sh_degree, float initial_opacity,
+                               float* params, int32_t* rest_per_channel) {
+  return guarded(ctx, [&] {
+    if (n < 0) throw Error(PXS_ERR_INVALID, "negative point count");
+    const int degree = std::max(0, std::min(3, static_cast<int>(sh_degree)));
+    const int S = (degree + 1) * (degree + 1) - 1;
+    if (rest_per_channel) *rest_per_channel = S;
+    if (n == 0 || params == nullptr) return;
+    if (points == nullptr) throw Error(PXS_ERR_INVALID, "points are null");
+    // the sampled nearest-neighbour spacing (GaussianCloud.cpp:206-227)
+    const int sample = std::min(n, 512);
+    const int stride = std::max(1, n / sample);
+    const int samples = (n + stride - 1) / stride;  // i = 0, stride, ... < n
+    float* d_points = ctx->image_b.reserve(static_cast<size_t>(n) * 3);
+    PXS_CUDA(cudaMemcpyAsync(d_points, points, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    double* d_near = ctx->seed_nearest.reserve(static_cast<size_t>(samples));
+    pxs::launch_seed_nearest(d_points, n, stride, samples, d_near, ctx->stream);
+    PXS_CUDA(cudaGetLastError());
+    std::vector<double> nearest(static_cast<size_t>(samples));
+    PXS_CUDA(cudaMemcpyAsync(nearest.data(), d_near, sizeof(double) * samples,
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    PXS_CUDA(cudaStreamSynchronize(ctx->stream));
+    double spacing = 0.0;
+    int counted = 0;
+    for (double d : nearest) {
+      if (d < 1e29) {
+        spacing += d;
+        ++counted;
+      }
+    }
+    spacing = counted > 0 ? spacing / counted : 0.01;
+    const double sigma = std::max(1e-4, spacing * 0.5);
+    const float log_sigma = static_cast<float>(std::log(sigma));
+    const float logit = std::log(std::max(1e-6f, initial_opacity) /
+                                 std::max(1e-6f, 1.f - initial_opacity));
+    const uint8_t* d_colors = nullptr;
+    if (colors != nullptr) {
+      uint8_t* dc = ctx->ingest_in.reserve(static_cast<size_t>(n) * 3);
+      PXS_CUDA(cudaMemcpyAsync(dc, colors, static_cast<size_t>(n) * 3, cudaMemcpyHostToDevice,
+                               ctx->stream));
+      d_colors = dc;
+    }
+    const size_t values = static_cast<size_t>(PXS_PARAM_COUNT(S)) * n;
+    float* d_params = ctx->params.reserve(values);
+    pxs::launch_seed_points(d_points, d_colors, n, S, log_sigma, logit, d_params, ctx->stream);
+    PXS_CUDA(cudaGetLastError());
+    PXS_CUDA(cudaMemcpyAsync(params, d_params, values * sizeof(float), cudaMemcpyDeviceToHost,
+                             ctx->stream));
     PXS_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }

@@ -195,3 +195,70 @@ void launch_pack_spz(const float* params, int n, int fractional_bits, int rest_s
 }
 
 }  // namespace pxs
+
+// ------------------------------------------------- initializeFromPointCloud
+//
+// GaussianCloud.cpp:199-257. The spacing estimate's O(samples^2) nearest-
+// neighbour search runs on the device, one thread per sampled point, with the
+// reference's arithmetic: float differences, the squared norm summed as
+// x^2 + (y^2 + z^2) (Eigen's unrolled 3-term reduction), its float square root
+// widened to double. The host sums the distances in order and takes the logs.
+namespace pxs {
+
+__global__ void __launch_bounds__(256)
+    k_seed_nearest(const float* __restrict__ points, int n, int stride, int samples,
+                   double* __restrict__ nearest) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= samples) return;
+  const int64_t i = (int64_t)s * stride;
+  const float xi = points[i * 3], yi = points[i * 3 + 1], zi = points[i * 3 + 2];
+  double best = 1e30;
+  for (int64_t j = 0; j < n; j += stride) {
+    if (j == i) continue;
+    const float dx = xi - points[j * 3], dy = yi - points[j * 3 + 1], dz = zi - points[j * 3 + 2];
+    const double d = (double)sqrtf(dx * dx + (dy * dy + dz * dz));
+    best = d < best ? d : best;  // std::min(best, d)
+  }
+  nearest[s] = best;
+}
+
+// One gaussian per point: position, isotropic log sigma, identity rotation,
+// the opacity logit, the DC colour from the point's 8-bit colour (or zero),
+// zero higher SH. Component-major with n gaussians per component.
+__global__ void __launch_bounds__(256)
+    k_seed_points(const float* __restrict__ points, const uint8_t* __restrict__ colors, int n,
+                  int S, float log_sigma, float logit, float* __restrict__ params) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const int64_t N = n;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    params[(PXS_C_POSITION + a) * N + g] = points[(int64_t)g * 3 + a];
+    params[(PXS_C_LOG_SCALE + a) * N + g] = log_sigma;
+    params[(PXS_C_DC + a) * N + g] =
+        colors != nullptr ? ((float)colors[(int64_t)g * 3 + a] / 255.0f - 0.5f) / kShC0 : 0.f;
+  }
+  params[(PXS_C_ROTATION + 0) * N + g] = 1.f;  // w
+  params[(PXS_C_ROTATION + 1) * N + g] = 0.f;
+  params[(PXS_C_ROTATION + 2) * N + g] = 0.f;
+  params[(PXS_C_ROTATION + 3) * N + g] = 0.f;
+  params[PXS_C_OPACITY * N + g] = logit;
+  for (int k = 0; k < 3 * S; ++k) params[(PXS_C_SH_REST + k) * N + g] = 0.f;
+}
+
+void launch_seed_nearest(const float* points, int n, int stride, int samples, double* nearest,
+                         cudaStream_t stream) {
+  if (samples <= 0) return;
+  count_launch();
+  k_seed_nearest<<<(samples + 255) / 256, 256, 0, stream>>>(points, n, stride, samples, nearest);
+}
+
+void launch_seed_points(const float* points, const uint8_t* colors, int n, int S,
+                        float log_sigma, float logit, float* params, cudaStream_t stream) {
+  if (n <= 0) return;
+  count_launch();
+  k_seed_points<<<(n + 255) / 256, 256, 0, stream>>>(points, colors, n, S, log_sigma, logit,
+                                                     params);
+}
+
+}  // namespace pxs

@@ -136,6 +136,12 @@ void launch_pack_splat(const float* params, int n, uint8_t* out, cudaStream_t st
 void launch_pack_spz(const float* params, int n, int fractional_bits, int rest_stored,
                      int rest_degree, uint8_t* out, cudaStream_t stream);
 
+// export.cu: initializeFromPointCloud's device parts
+void launch_seed_nearest(const float* points, int n, int stride, int samples, double* nearest,
+                         cudaStream_t stream);
+void launch_seed_points(const float* points, const uint8_t* colors, int n, int S,
+                        float log_sigma, float logit, float* params, cudaStream_t stream);
+
 // ingest.cu: downscaleToWidth's box filter (and the /255 to float) on the device
 void launch_downscale(const uint8_t* src, int width, int height, int out_width, int out_height,
                       uint8_t* out_bytes, float* out_linear, cudaStream_t stream);

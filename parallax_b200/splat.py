@@ -512,6 +512,26 @@ def export_cloud(cloud: GaussianCloud, fmt: str = "ply", fractional_bits: int = 
     return data
 
 
+def initialize_from_points(points: np.ndarray, colors: Optional[np.ndarray] = None,
+                           sh_degree: int = 0, initial_opacity: float = 0.1,
+                           ctx: Optional[Context] = None) -> GaussianCloud:
+    """initializeFromPointCloud (GaussianCloud.cpp:199-257) with the spacing
+    search on the device. points: (n, 3) float32; colors: (n, 3) uint8 or None."""
+    ctx = ctx or default_context()
+    pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+    n = pts.shape[0]
+    cols = None if colors is None else np.ascontiguousarray(colors, dtype=np.uint8).reshape(-1, 3)
+    rest = ct.c_int32()
+    ctx.check(lib().pxs_initialize_from_points(ctx.handle, None, None, n, sh_degree,
+                                               ct.c_float(initial_opacity), None, ct.byref(rest)))
+    out = np.zeros((A.param_count(rest.value), n), dtype=np.float32)
+    ctx.check(lib().pxs_initialize_from_points(
+        ctx.handle, pts.ctypes.data if n else None, None if cols is None else cols.ctypes.data,
+        n, sh_degree, ct.c_float(initial_opacity), out.ctypes.data if n else None,
+        ct.byref(rest)))
+    return GaussianCloud(out, max(0, min(3, sh_degree)), rest.value)
+
+
 def downscale_to_width(rgb: np.ndarray, width: int, height: int, target_width: int,
                        ctx: Optional[Context] = None):
     """downscaleToWidth (ImageIo.cpp:300-337) on the device: (bytes H*W*3 uint8,

@@ -60,3 +60,33 @@ def test_trainer_ingests_frames_at_its_view_size():
         t.ingest_images([0], [np.zeros(1280 * 800 * 3, np.uint8)], [(1280, 800)])
     for x in (t, a):
         x.close()
+
+
+def reference_seed(points, colors, sh_degree, opacity):
+    lib = O.ref()
+    lib.ref_initialize_from_points.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int,
+                                               ct.c_float, ct.c_void_p]
+    n = points.shape[0]
+    rest = (min(3, max(0, sh_degree)) + 1) ** 2 - 1
+    out = np.zeros(((14 + 3 * rest), n), np.float32)
+    got = lib.ref_initialize_from_points(points.ctypes.data,
+                                         None if colors is None else colors.ctypes.data, n,
+                                         sh_degree, opacity, out.ctypes.data)
+    assert got == n
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,sh,with_colors", [(3000, 0, True), (700, 3, True), (20000, 1, False),
+                                               (2, 2, True), (1, 0, True)])
+def test_seed_matches_the_reference(n, sh, with_colors):
+    """initializeFromPointCloud (GaussianCloud.cpp:199-257): the spacing search
+    on the device, bit-exact."""
+    rs = np.random.default_rng(n + sh)
+    points = np.ascontiguousarray(rs.normal(0, 1, (n, 3)).astype(np.float32))
+    colors = np.ascontiguousarray(rs.integers(0, 256, (n, 3), dtype=np.uint8)) \
+        if with_colors else None
+    ours = px.initialize_from_points(points, colors, sh, 0.1)
+    ref = reference_seed(points, colors, sh, 0.1)
+    assert ours.params.shape == ref.shape
+    assert np.array_equal(ours.params.view(np.uint32), ref.view(np.uint32))
