@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
 // multiply-add per channel (fma.rn.f32x2), which differs from the separate
 // multiply and add by at most one rounding per entry. A pixel that does not
 // take an entry adds T * 0 * colour = 0.
-template <bool kCount>
+template <bool kCount, bool kBits>
 __global__ void __launch_bounds__(TileGeom<2>::kThreads)
     k_forward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
@@ -183,15 +183,15 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
   };
   for (int base = info.range.x; base < info.range.y; base += kBatch) {
     const bool all_done = __syncthreads_and(done0 && done1);
-    if (block_bits != nullptr) {
+    if (kBits) {
       write_bits();
       prev_n = 0;
     }
     if (all_done) break;
-    if (block_bits != nullptr) __syncthreads();  // the bits are read before they are cleared
+    if (kBits) __syncthreads();  // the bits are read before they are cleared
     const int n = min(kBatch, info.range.y - base);
     for (int i = threadIdx.x; i < n; i += kThreads) {
-      if (block_bits != nullptr) {
+      if (kBits) {
 #pragma unroll
         for (int w = 0; w < TileGeom<2>::kWarps; ++w) s_took[w][i] = 0;
       }
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
         const bool c1 = in1 && !(a1 < min_alpha);
         if (!(c0 || c1)) continue;
         if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
-        if (block_bits != nullptr) s_took[warp][j] = 1;  // same value from every lane
+        if (kBits) s_took[warp][j] = 1;  // same value from every lane
         const float4 c = s_col[j];
         const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
         acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
     prev_base = base;
     prev_n = n;
   }
-  if (block_bits != nullptr && prev_n > 0) {  // the last batch, when the list ran out
+  if (kBits && prev_n > 0) {  // the last batch, when the list ran out
     __syncthreads();
     write_bits();
   }
@@ -304,8 +304,13 @@ void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, co
                             total_tiles, rgb, T, last, stream, counts);
       break;
     default:
-      k_forward_x2<kCount><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts, bits);
+      if (bits != nullptr)
+        k_forward_x2<kCount, true><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
+            ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts, bits);
+      else
+        k_forward_x2<kCount, false><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
+            ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts,
+            nullptr);
   }
 }
 
