@@ -160,11 +160,14 @@ __global__ void __launch_bounds__(1024)
   if (threadIdx.x == 0) n_chunks[0] = min(carry, max_chunks);
 }
 
-// Per-warp column counts of one chunk into s_cnt [kWarps][tiles_x] (zeroed by
-// the caller); lanes prefetch their records' rects first.
+// Per-warp column counts of one chunk into s_cnt [kWarps][max_tiles_x]
+// (zeroed by the caller): each record adds +1 at its first column and -1 past
+// its last (two shared-memory atomics however wide it is), then each warp's
+// row is prefix-summed over the columns. Lanes prefetch their records' rects.
 __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32_t* __restrict__ rec_slots,
                                                     const uint2* __restrict__ rect, int max_tiles_x,
-                                                    int32_t* s_cnt, uint32_t (&slot)[kPerLane],
+                                                    int tiles_x, int32_t* s_cnt,
+                                                    uint32_t (&slot)[kPerLane],
                                                     uint32_t (&xr)[kPerLane]) {
   const int w = warp_id(), lane = lane_id();
   const int w_begin = ch.y + w * (kChunk / kWarps);
@@ -178,11 +181,29 @@ __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32
       xr[k] = rect[slot[k]].x;
     }
   }
+  int32_t* row = s_cnt + w * max_tiles_x;
 #pragma unroll
   for (int k = 0; k < kPerLane; ++k) {
     const int x0 = xr[k] & 0xFFFF, x1 = xr[k] >> 16;
-    for (int c = x0; c <= x1; ++c) atomicAdd(&s_cnt[w * max_tiles_x + c], 1);
+    if (x1 >= x0) {
+      atomicAdd(&row[x0], 1);
+      if (x1 + 1 < tiles_x) atomicAdd(&row[x1 + 1], -1);
+    }
   }
+  __syncwarp();
+  int carry = 0;
+  for (int c0 = 0; c0 < tiles_x; c0 += 32) {
+    const int c = c0 + lane;
+    int v = c < tiles_x ? row[c] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int n = __shfl_up_sync(kFull, v, o);
+      if (lane >= o) v += n;
+    }
+    if (c < tiles_x) row[c] = carry + v;
+    carry += __shfl_sync(kFull, v, 31);
+  }
+  __syncwarp();
 }
 
 // Per chunk: how many of its records cover each column.
@@ -200,7 +221,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
   __syncthreads();
   uint32_t slot[kPerLane], xr[kPerLane];
-  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, s_cnt, slot, xr);
+  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, s_cnt, slot, xr);
   __syncthreads();
   for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
     int total = 0;
@@ -322,7 +343,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   __syncthreads();
   uint32_t slot[kPerLane], xr[kPerLane];
-  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, s_cnt, slot, xr);
+  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, s_cnt, slot, xr);
   __syncthreads();
   // per-column totals, then their exclusive scan: each column's stage start
   const int per = (tiles_x + blockDim.x - 1) / blockDim.x;

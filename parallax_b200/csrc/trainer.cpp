@@ -952,15 +952,18 @@ int pxs_trainer_ingest_images(pxs_trainer* t, int32_t n, const int32_t* view_ids
       const size_t in_bytes = static_cast<size_t>(widths[i]) * heights[i] * 3;
       if (in_bytes == 0) continue;
       if (frames[i] == nullptr) throw Error(PXS_ERR_INVALID, "frame is null");
+      // the staging buffer is reused by the next frame: the stream orders the
+      // next copy after this frame's downscale; it is grown only when idle
+      if (in_bytes > t->ingest_in.capacity()) PXS_CUDA(cudaStreamSynchronize(t->stream));
       uint8_t* d_in = t->ingest_in.reserve(in_bytes);
       PXS_CUDA(cudaMemcpyAsync(d_in, frames[i], in_bytes, cudaMemcpyHostToDevice, t->stream));
       pxs::launch_downscale(d_in, widths[i], heights[i], w, h, nullptr,
                             t->images.get() + t->image_offset[static_cast<size_t>(id)] * 3,
                             t->stream);
       PXS_CUDA(cudaGetLastError());
-      // the staging buffer is reused by the next frame: wait for this one
-      PXS_CUDA(cudaStreamSynchronize(t->stream));
     }
+    // the frames may be released once the call returns
+    PXS_CUDA(cudaStreamSynchronize(t->stream));
   });
 }
 
