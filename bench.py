@@ -55,6 +55,9 @@ def parse_args():
     p.add_argument("--workload", default="c4")
     p.add_argument("--views", type=int, default=0,
                    help="views per step (default: the workload's); a smaller case for profiling")
+    p.add_argument("--pool", type=int, default=0,
+                   help="use only the first N cameras of the pool (smaller device footprint, "
+                        "for profiler captures); 0 = the workload's pool")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -304,6 +307,8 @@ def run_ours(args):
     w = WORKLOADS[args.workload]
     V = args.views or w["views_per_step"]
     truth, start, views = workload_scene(args.workload)
+    if args.pool > 0:
+        views = views[:args.pool]
     P = px.param_count(start.rest_per_channel)
     N = start.count
 

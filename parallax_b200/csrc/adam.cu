@@ -5,6 +5,8 @@
 // thread per gaussian so the quaternion can be renormalised in registers.
 // Compiled with -fmad=false: with IEEE division and square root the update is
 // bit-identical to the reference's for identical gradients.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -36,17 +38,38 @@ __global__ void __launch_bounds__(256)
   // positionLearningRate (SplatTrainer.cpp:200-208) ends with "* extent": with
   // several scenes lr[0] holds the rest and each gaussian its scene's extent
   const float lr_position = position_scale != nullptr ? s.lr[0] * position_scale[g] : s.lr[0];
-  for (int c = 0; c < P; ++c) {
-    if (c >= PXS_C_ROTATION && c < PXS_C_ROTATION + 4) continue;
-    const int group = c < 3 ? 0 : (c < 6 ? 1 : (c == PXS_C_OPACITY ? 3 : (c < 14 ? 4 : 5)));
-    const int64_t i = (int64_t)c * n + g;
-    float mm = m[i], vv = v[i];
-    params[i] += adam_delta(mm, vv, grads[i], group == 0 ? lr_position : s.lr[group], s.beta1,
-                            s.beta2, s.epsilon, s.correction1, s.correction2);
-    m[i] = mm;
-    v[i] = vv;
-    if (zero_grads) grads[i] = 0.f;
-  }
+  // channels [c0, c0 + K) with learning rate lr(c): every load of the group
+  // is issued before its first store, so K channels' loads are in flight at once
+  auto update = [&](auto K, int c0, auto lr_of) {
+    constexpr int k = decltype(K)::value;
+    float pp[k], gg[k], mm[k], vv[k];
+#pragma unroll
+    for (int j = 0; j < k; ++j) {
+      const int64_t i = (int64_t)(c0 + j) * n + g;
+      pp[j] = params[i];
+      gg[j] = grads[i];
+      mm[j] = m[i];
+      vv[j] = v[i];
+    }
+#pragma unroll
+    for (int j = 0; j < k; ++j) {
+      const int64_t i = (int64_t)(c0 + j) * n + g;
+      params[i] = pp[j] + adam_delta(mm[j], vv[j], gg[j], lr_of(c0 + j), s.beta1, s.beta2,
+                                     s.epsilon, s.correction1, s.correction2);
+      m[i] = mm[j];
+      v[i] = vv[j];
+      if (zero_grads) grads[i] = 0.f;
+    }
+  };
+  using Six = std::integral_constant<int, 6>;
+  using Four = std::integral_constant<int, 4>;
+  using One = std::integral_constant<int, 1>;
+  // position and log-scale, then opacity and dc, then the SH rest
+  update(Six{}, 0, [&](int c) { return c < 3 ? lr_position : s.lr[1]; });
+  update(Four{}, PXS_C_OPACITY, [&](int c) { return c == PXS_C_OPACITY ? s.lr[3] : s.lr[4]; });
+  int c = PXS_C_SH_REST;
+  for (; c + 4 <= P; c += 4) update(Four{}, c, [&](int) { return s.lr[5]; });
+  for (; c < P; ++c) update(One{}, c, [&](int) { return s.lr[5]; });
   float q[4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {

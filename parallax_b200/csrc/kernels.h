@@ -33,6 +33,7 @@ struct ScanScratch {
 void launch_project(const float* params, int N, int S, int64_t slot_stride,
                     const ViewDesc* views, int n_views, const ProjectedSoA& out,
                     cudaStream_t stream);
+void configure_param_grads_kernel();  // once per device, outside graph capture
 void launch_param_grads(const float* params, int N, int S, int64_t slot_stride,
                         const ViewDesc* views, int n_views, const uint32_t* depth_key,
                         const float4* conic_op, const float4* color, const ScreenGrad* screen,

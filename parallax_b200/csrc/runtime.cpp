@@ -98,6 +98,7 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   if (!configured_) {
     configure_loss_kernel();
     configure_bin_kernels();
+    configure_param_grads_kernel();
     PXS_CUDA(cudaGetLastError());
     configured_ = true;
   }
