@@ -3,14 +3,17 @@
 //
 // photometricLoss / meanSsim (SplatRaster.cpp:582-738) run 13 separable
 // blurs per channel over whole-image planes. Here a CTA owns a 32x16 output
-// tile and stages the rendered and target images over a 10-pixel halo (two
-// stacked 11-tap blurs): it blurs the five statistic planes (x, y, xx, yy, xy)
-// onto a 5-pixel halo, forms the SSIM map and its three partials there
-// (zero outside the image, as the reference's zero-padded adjoint requires),
-// blurs the five partial planes back onto the tile and writes dL/drgb.
-// Each blur pass is register-blocked: a thread loads a strip once and slides
-// the 11 taps along it. Sums run in the reference's tap order (fused
-// multiply-adds allowed); the scalar totals are accumulated in double.
+// tile and stages each channel of the rendered and target images over a
+// 10-pixel halo (two stacked 11-tap blurs): it blurs the five statistic
+// planes (x, y, xx, yy, xy) onto a 5-pixel halo, forms the SSIM map and its
+// partials there (zero outside the image, as the reference's zero-padded
+// adjoint requires), blurs them back onto the tile and writes dL/drgb. The
+// reference blurs five partial planes back; by linearity of the blur the three
+// without a pixel factor are summed first, so three planes are blurred (equal
+// in exact arithmetic, within FP32 rounding otherwise). Each blur pass is
+// register-blocked: a thread loads a strip once and slides the 11 taps along
+// it. Sums run in the reference's tap order (fused multiply-adds allowed);
+// the scalar totals are accumulated in double.
 #include <cstdio>
 #include <exception>
 #include <mutex>
@@ -28,10 +31,10 @@ constexpr int SW = TW + 10, SH = TH + 10;  // statistics region
 constexpr int kThreads = 256;
 
 struct LossSmem {
-  float in_r[3][IH][IW];   // rendered, all channels
-  float in_t[3][IH][IW];   // target
-  float hb[5][IH][SW];     // horizontal blur of the five products / of the partials
-  float st[5][SH][SW];     // statistics, then in place the five partial planes
+  float in_r[IH][IW];      // rendered, the current channel
+  float in_t[IH][IW];      // target
+  float hb[5][IH][SW];     // horizontal blur of the five products / of the three partials
+  float st[3][SH][SW];     // the three partial planes
 };
 
 }  // namespace
@@ -40,7 +43,7 @@ struct LossSmem {
 // With `flat`, the grid is one-dimensional over every view's own output tiles,
 // view after view (views of different sizes waste no CTAs); otherwise the
 // grid is (tiles across, tiles down, view) for the largest view.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
     k_loss(const float* __restrict__ rendered, const float* __restrict__ target,
            const ViewDesc* __restrict__ views, int n_views, LossParams lp,
            float* __restrict__ grad_out, double* __restrict__ sums, int flat) {
@@ -71,28 +74,6 @@ __global__ void __launch_bounds__(kThreads)
   const float* timg = target + vd.target_offset * 3;
   const int tid = threadIdx.x;
 
-  // stage both images over the input region, zero outside
-  for (int q = tid; q < IH * IW; q += kThreads) {
-    const int lx = q % IW, ly = q / IW;
-    const int X = ox - 10 + lx, Y = oy - 10 + ly;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
-    if (X >= 0 && X < W && Y >= 0 && Y < H) {
-      const int64_t o = ((int64_t)Y * W + X) * 3;
-      a0 = rimg[o];
-      a1 = rimg[o + 1];
-      a2 = rimg[o + 2];
-      b0 = timg[o];
-      b1 = timg[o + 1];
-      b2 = timg[o + 2];
-    }
-    sm.in_r[0][ly][lx] = a0;
-    sm.in_r[1][ly][lx] = a1;
-    sm.in_r[2][ly][lx] = a2;
-    sm.in_t[0][ly][lx] = b0;
-    sm.in_t[1][ly][lx] = b1;
-    sm.in_t[2][ly][lx] = b2;
-  }
-  __syncthreads();
 
   const float w = lp.ssim_weight;
   // 1 / values and 1 / (pixels * 3) of photometricLoss and meanSsim: equal
@@ -103,6 +84,22 @@ __global__ void __launch_bounds__(kThreads)
   const bool want_ssim = lp.mode == 1 || w > 0.f;
 
   for (int c = 0; c < 3; ++c) {
+    // stage channel c of both images over the input region, zero outside
+    // (one channel at a time keeps three CTAs per SM; the other channels'
+    // bytes of the same lines come back from L2)
+    for (int q = tid; q < IH * IW; q += kThreads) {
+      const int lx = q % IW, ly = q / IW;
+      const int X = ox - 10 + lx, Y = oy - 10 + ly;
+      float a = 0.f, b = 0.f;
+      if (X >= 0 && X < W && Y >= 0 && Y < H) {
+        const int64_t o = ((int64_t)Y * W + X) * 3 + c;
+        a = rimg[o];
+        b = timg[o];
+      }
+      sm.in_r[ly][lx] = a;
+      sm.in_t[ly][lx] = b;
+    }
+    __syncthreads();
     if (want_ssim) {
       // horizontal blur of the five products over every input row, onto the
       // statistics columns; a thread slides the 11 taps over 6 outputs
@@ -112,8 +109,8 @@ __global__ void __launch_bounds__(kThreads)
         float xs[HS + 10], ys[HS + 10], xx[HS + 10], yy[HS + 10], xy[HS + 10];
 #pragma unroll
         for (int k = 0; k < HS + 10; ++k) {
-          xs[k] = sm.in_r[c][r][col0 + k];
-          ys[k] = sm.in_t[c][r][col0 + k];
+          xs[k] = sm.in_r[r][col0 + k];
+          ys[k] = sm.in_t[r][col0 + k];
           xx[k] = xs[k] * xs[k];
           yy[k] = ys[k] * ys[k];
           xy[k] = xs[k] * ys[k];
@@ -183,17 +180,18 @@ __global__ void __launch_bounds__(kThreads)
             mu_x = 0.f;
             mu_y = 0.f;
           }
-          sm.st[0][r][col] = t_mu;
+          // dL/dx = blur(t_mu) + 2x blur(t_var) - 2 blur(t_var mu_x)
+          //        + y blur(t_cov) - blur(t_cov mu_y); the blur is linear, so
+          // the three terms without a pixel factor are blurred as one plane
+          sm.st[0][r][col] = t_mu - 2.f * t_var * mu_x - t_cov * mu_y;
           sm.st[1][r][col] = t_var;
-          sm.st[2][r][col] = t_var * mu_x;
-          sm.st[3][r][col] = t_cov;
-          sm.st[4][r][col] = t_cov * mu_y;
+          sm.st[2][r][col] = t_cov;
         }
       }
       __syncthreads();
       // horizontal blur of the partials onto the tile's columns, 8 per thread
       constexpr int HS2 = 8;
-      for (int item = tid; item < 5 * SH * (TW / HS2); item += kThreads) {
+      for (int item = tid; item < 3 * SH * (TW / HS2); item += kThreads) {
         const int p = item / (SH * (TW / HS2));
         const int rem = item % (SH * (TW / HS2));
         const int r = rem / (TW / HS2), col0 = (rem % (TW / HS2)) * HS2;
@@ -214,10 +212,10 @@ __global__ void __launch_bounds__(kThreads)
     constexpr int VS2 = 2;
     for (int item = tid; item < TW * (TH / VS2); item += kThreads) {
       const int col = item % TW, r0 = (item / TW) * VS2;
-      float B[5][VS2];
+      float B[3][VS2];
       if (want_ssim) {
 #pragma unroll
-        for (int p = 0; p < 5; ++p) {
+        for (int p = 0; p < 3; ++p) {
           float hv[VS2 + 10];
 #pragma unroll
           for (int k = 0; k < VS2 + 10; ++k) hv[k] = sm.hb[p][r0 + k][col];
@@ -235,15 +233,13 @@ __global__ void __launch_bounds__(kThreads)
         const int r = r0 + o;
         const int X = ox + col, Y = oy + r;
         if (X >= W || Y >= H) continue;
-        const float x = sm.in_r[c][r + 10][col + 10];
-        const float y = sm.in_t[c][r + 10][col + 10];
+        const float x = sm.in_r[r + 10][col + 10];
+        const float y = sm.in_t[r + 10][col + 10];
         float d = 0.f;
         if (want_ssim) {
           d = B[0][o];
           d += 2.f * x * B[1][o];
-          d -= 2.f * B[2][o];
-          d += y * B[3][o];
-          d -= B[4][o];
+          d += y * B[2][o];
         }
         const int64_t oidx = (pix0 + (int64_t)Y * W + X) * 3 + c;
         if (lp.mode == 1) {
