@@ -24,6 +24,7 @@ constexpr uint32_t kCulledKey = 0xFFFFFFFFu;
 
 // Widest image, in tiles, the row-binning kernels stage in shared memory.
 constexpr int kMaxTilesX = 2048;
+constexpr int kMaxTilesY = 2048;
 
 // Everything a kernel needs to know about one view of a batch.
 struct ViewDesc {
@@ -37,7 +38,7 @@ struct ViewDesc {
   float min_alpha;
   float transmittance_cutoff;
   float screen_dilation;
-  int32_t loss_tile_offset;  // first 32x16 tile of this view in the loss kernel's flat grid
+  int32_t loss_tile_offset;  // first output tile of this view in the loss kernel's flat grid
   int64_t target_offset;     // first pixel of this view's target image
   // the gaussians this view renders: [gauss_offset, gauss_offset + gauss_count)
   // of the parameter arrays; slot v * slot_stride + i holds gaussian

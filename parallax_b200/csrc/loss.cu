@@ -2,7 +2,7 @@
 // gradient, fused into one shared-memory tiled kernel.
 //
 // photometricLoss / meanSsim (SplatRaster.cpp:582-738) run 13 separable
-// blurs per channel over whole-image planes. Here a CTA owns a 32x16 output
+// blurs per channel over whole-image planes. Here a CTA owns a 32x32 output
 // tile and stages each channel of the rendered and target images over a
 // 10-pixel halo (two stacked 11-tap blurs): it blurs the five statistic
 // planes (x, y, xx, yy, xy) onto a 5-pixel halo, forms the SSIM map and its
@@ -25,7 +25,7 @@
 namespace pxs {
 namespace {
 
-constexpr int TW = 32, TH = 16;
+constexpr int TW = 32, TH = 32;
 constexpr int IW = TW + 20, IH = TH + 20;  // input region
 constexpr int SW = TW + 10, SH = TH + 10;  // statistics region
 constexpr int kThreads = 256;
@@ -43,7 +43,7 @@ struct LossSmem {
 // With `flat`, the grid is one-dimensional over every view's own output tiles,
 // view after view (views of different sizes waste no CTAs); otherwise the
 // grid is (tiles across, tiles down, view) for the largest view.
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 2)
     k_loss(const float* __restrict__ rendered, const float* __restrict__ target,
            const ViewDesc* __restrict__ views, int n_views, LossParams lp,
            float* __restrict__ grad_out, double* __restrict__ sums, int flat) {
@@ -136,8 +136,8 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       __syncthreads();
       // vertical blur -> statistics, then the SSIM map and its partials in
-      // place; a thread takes one column and 4 consecutive rows
-      constexpr int VS = 4;
+      // place; a thread takes one column and 6 consecutive rows
+      constexpr int VS = 6;
       constexpr int VSEG = (SH + VS - 1) / VS;
       for (int item = tid; item < SW * VSEG; item += kThreads) {
         const int col = item % SW, r0 = (item / SW) * VS;
@@ -208,8 +208,8 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       __syncthreads();
     }
-    // vertical blur and the gradient, one column and 2 rows per thread
-    constexpr int VS2 = 2;
+    // vertical blur and the gradient, one column and 4 rows per thread
+    constexpr int VS2 = 4;
     for (int item = tid; item < TW * (TH / VS2); item += kThreads) {
       const int col = item % TW, r0 = (item / TW) * VS2;
       float B[3][VS2];
