@@ -5,14 +5,19 @@
 // is near to far. Sorting the (tile, splat) pairs themselves moves every pair
 // through memory once per radix pass. Here the rectangle structure is used
 // instead:
-//   1. each visible splat (in depth order) emits one record per tile row it
-//      covers -- (global row id, slot), about one seventh as many as pairs;
-//   2. one stable radix pass groups the records by row, keeping depth order;
-//   3. each row is cut into chunks of 1024 records; one CTA per chunk counts,
+//   1. each visible splat has one record per tile row it covers (about one
+//      seventh as many as pairs), wanted grouped by row and near to far
+//      within a row: each view's depth-sorted slots are cut into chunks of
+//      512; a CTA per chunk counts, per tile row, the splats covering it; an
+//      exclusive scan of the counts in (row, chunk) order gives each chunk
+//      its base in each row, and the chunk writes its records there (the
+//      ranking of step 3 with rows for columns) -- a stable counting sort by
+//      row with no sort pass;
+//   2. each row is cut into chunks of 1024 records; one CTA per chunk counts,
 //      per column, the records covering it; a per-row pass turns those into
 //      each chunk's base within every tile of the row and the tiles' lengths;
 //      an exclusive scan over the tiles gives the tile ranges;
-//   4. one CTA per chunk walks its records again, 32 at a time per warp: each
+//   3. one CTA per chunk walks its records again, 32 at a time per warp: each
 //      lane sets its bit in a per-column bitmap for every column its splat
 //      covers, and the pair's place among the chunk's pairs of that column is
 //      the column's running base plus the number of earlier lanes in the
@@ -37,73 +42,6 @@ __device__ __forceinline__ int view_of_row(const ViewDesc* __restrict__ views, i
 }
 
 }  // namespace
-
-// Rows covered by the i-th nearest slot of each view (0 when culled).
-__global__ void k_gather_row_counts(const uint32_t* __restrict__ sorted_slots,
-                                    const int32_t* __restrict__ tile_count,
-                                    const uint2* __restrict__ rect, int64_t n,
-                                    int32_t* __restrict__ counts) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t slot = sorted_slots[i];
-  int rows = 0;
-  if (tile_count[slot] > 0) {
-    const uint2 r = rect[slot];
-    rows = (int)(r.y >> 16) - (int)(r.y & 0xFFFF) + 1;
-  }
-  counts[i] = rows;
-}
-
-// One record (global row id, slot) per covered row, in depth order. A warp
-// emits the records of 32 consecutive slots together (coalesced writes; each
-// lane finds the slot owning its output position by a binary search).
-__global__ void __launch_bounds__(256)
-    k_emit_rows(const uint32_t* __restrict__ sorted_slots, const int32_t* __restrict__ counts,
-                const int64_t* __restrict__ offsets, const uint2* __restrict__ rect,
-                const ViewDesc* __restrict__ views, int64_t slot_stride, int64_t n,
-                uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int64_t capacity,
-                uint32_t sentinel_row, int32_t* __restrict__ overflow) {
-  const int lane = lane_id();
-  const int64_t first = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) - lane;
-  if (first >= n) return;
-  const int64_t i = first + lane;
-  const bool valid = i < n;
-  const int cnt = valid ? counts[i] : 0;
-  const int64_t off = valid ? offsets[i] : (int64_t)-1;
-  const int64_t warp_begin = __shfl_sync(kFull, off, 0);
-  const int last_valid = min(31, (int)(n - 1 - first));
-  const int64_t warp_end = __shfl_sync(kFull, off + cnt, last_valid);
-  if (__any_sync(kFull, valid && cnt > 0 && off + cnt > capacity) && lane == 0)
-    atomicExch(overflow, 1);
-  uint32_t slot = 0, row0 = 0;
-  if (valid && cnt > 0) {
-    slot = sorted_slots[i];
-    const uint2 r = rect[slot];
-    row0 = (uint32_t)views[slot / slot_stride].row_offset + (r.y & 0xFFFF);
-  }
-  for (int64_t base = warp_begin; base < warp_end; base += 32) {
-    const int64_t out = base + lane;
-    int owner = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-      const int cand = owner + step;
-      const int64_t cand_off = __shfl_sync(kFull, off, cand & 31);
-      if (cand <= last_valid && cand_off <= out) owner = cand;
-    }
-    const int64_t o_off = __shfl_sync(kFull, off, owner);
-    const int o_cnt = __shfl_sync(kFull, cnt, owner);
-    const uint32_t o_slot = __shfl_sync(kFull, slot, owner);
-    const uint32_t o_row0 = __shfl_sync(kFull, row0, owner);
-    if (out >= warp_end || out >= capacity) continue;
-    if (o_off + o_cnt > capacity) {  // does not fit: a sentinel past every row
-      keys[out] = sentinel_row;
-      vals[out] = 0u;
-      continue;
-    }
-    keys[out] = o_row0 + (uint32_t)(out - o_off);
-    vals[out] = o_slot;
-  }
-}
 
 // Rows are cut into chunks of at most kChunk records so the work balances
 // whatever the rows' lengths. chunks[c] = (row, begin, end); n_chunks[0] is
@@ -160,10 +98,41 @@ __global__ void __launch_bounds__(1024)
   if (threadIdx.x == 0) n_chunks[0] = min(carry, max_chunks);
 }
 
-// Per-warp column counts of one chunk into s_cnt [kWarps][max_tiles_x]
-// (zeroed by the caller): each record adds +1 at its first column and -1 past
-// its last (two shared-memory atomics however wide it is), then each warp's
-// row is prefix-summed over the columns. Lanes prefetch their records' rects.
+// Per-warp counts of the lanes' ranges range[k] = lo | hi << 16 (empty when
+// hi < lo) over the columns of `row` (zeroed by the caller, `extent` wide):
+// each range adds +1 at lo and -1 past hi (two shared-memory atomics however
+// wide it is), then the warp prefix-sums its row.
+template <int K>
+__device__ __forceinline__ void warp_range_counts(const uint32_t (&range)[K], int extent,
+                                                  int32_t* row) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int lo = range[k] & 0xFFFF, hi = range[k] >> 16;
+    if (hi >= lo) {
+      atomicAdd(&row[lo], 1);
+      if (hi + 1 < extent) atomicAdd(&row[hi + 1], -1);
+    }
+  }
+  __syncwarp();
+  int carry = 0;
+  for (int c0 = 0; c0 < extent; c0 += 32) {
+    const int c = c0 + lane;
+    int v = c < extent ? row[c] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int n = __shfl_up_sync(kFull, v, o);
+      if (lane >= o) v += n;
+    }
+    if (c < extent) row[c] = carry + v;
+    carry += __shfl_sync(kFull, v, 31);
+  }
+  __syncwarp();
+}
+
+// Per-warp column counts of one chunk of row records into s_cnt
+// [kWarps][max_tiles_x] (zeroed by the caller); lanes prefetch their records'
+// rects first.
 __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32_t* __restrict__ rec_slots,
                                                     const uint2* __restrict__ rect, int max_tiles_x,
                                                     int tiles_x, int32_t* s_cnt,
@@ -181,29 +150,7 @@ __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32
       xr[k] = rect[slot[k]].x;
     }
   }
-  int32_t* row = s_cnt + w * max_tiles_x;
-#pragma unroll
-  for (int k = 0; k < kPerLane; ++k) {
-    const int x0 = xr[k] & 0xFFFF, x1 = xr[k] >> 16;
-    if (x1 >= x0) {
-      atomicAdd(&row[x0], 1);
-      if (x1 + 1 < tiles_x) atomicAdd(&row[x1 + 1], -1);
-    }
-  }
-  __syncwarp();
-  int carry = 0;
-  for (int c0 = 0; c0 < tiles_x; c0 += 32) {
-    const int c = c0 + lane;
-    int v = c < tiles_x ? row[c] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int n = __shfl_up_sync(kFull, v, o);
-      if (lane >= o) v += n;
-    }
-    if (c < tiles_x) row[c] = carry + v;
-    carry += __shfl_sync(kFull, v, 31);
-  }
-  __syncwarp();
+  warp_range_counts(xr, tiles_x, s_cnt + w * max_tiles_x);
 }
 
 // Per chunk: how many of its records cover each column.
@@ -308,6 +255,127 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* tot
   return before;
 }
 
+// The chunk's layout from the per-warp counts in s_cnt [kWarps][stride] over
+// `extent` columns: per column its pair total (col_count), its start among
+// the chunk's staged pairs (col_start) and the list position of its first
+// pair (col_dst = dst_of(c)); the per-warp counts become per-warp bases in
+// place. Returns whether the chunk's pairs fit a stage of `stage_cap`.
+template <typename DstOf>
+__device__ __forceinline__ bool chunk_layout(int32_t* s_cnt, int stride, int extent,
+                                             int stage_cap, int* s_warp, int32_t* col_count,
+                                             int32_t* col_start, int64_t* col_dst,
+                                             DstOf dst_of) {
+  const int per = (extent + blockDim.x - 1) / blockDim.x;
+  const int c_begin = min(extent, (int)threadIdx.x * per);
+  const int c_end = min(extent, c_begin + per);
+  int mine = 0;
+  for (int c = c_begin; c < c_end; ++c) {
+    int t = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) t += s_cnt[k * stride + c];
+    col_count[c] = t;
+    mine += t;
+  }
+  int total = 0;
+  int run_start = block_exclusive_scan(mine, s_warp, &total);
+  for (int c = c_begin; c < c_end; ++c) {
+    col_start[c] = run_start;
+    col_dst[c] = dst_of(c);
+    // per warp, where its pairs of this column begin among the chunk's pairs
+    int run = run_start;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) {
+      const int t = s_cnt[k * stride + c];
+      s_cnt[k * stride + c] = run;
+      run += t;
+    }
+    run_start += col_count[c];
+  }
+  __syncthreads();
+  return total <= stage_cap;  // block-uniform
+}
+
+// Each warp places its lanes' payloads, 32 at a time, on every column of their
+// ranges: a lane sets its bit in the warp's per-column bitmap, and its place
+// among the chunk's pairs of the column is the warp's running base there plus
+// the number of earlier lanes in the bitmap. Staged pairs go to `stage`,
+// grouped by column; otherwise straight to out[col_dst + rank] below capacity.
+template <int K>
+__device__ __forceinline__ void warp_range_expand(const uint32_t (&range)[K],
+                                                  const uint32_t (&payload)[K], int32_t* base,
+                                                  uint32_t* bitmap, bool staged,
+                                                  uint32_t* stage, const int32_t* col_start,
+                                                  const int64_t* col_dst, int64_t capacity,
+                                                  uint32_t* __restrict__ out) {
+  const int lane = lane_id();
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int lo = range[k] & 0xFFFF, hi = range[k] >> 16;
+    for (int c = lo; c <= hi; ++c) atomicOr(&bitmap[c], 1u << lane);
+    __syncwarp();
+    for (int c = lo; c <= hi; ++c) {
+      const int pos = base[c] + __popc(bitmap[c] & lt);  // among the chunk's pairs
+      if (staged) {
+        stage[pos] = payload[k];
+      } else {
+        const int64_t dst = col_dst[c] + (pos - col_start[c]);
+        if (dst < capacity) out[dst] = payload[k];
+      }
+    }
+    __syncwarp();
+    const int wlo = __reduce_min_sync(kFull, hi >= lo ? lo : (1 << 30));
+    const int whi = __reduce_max_sync(kFull, hi >= lo ? hi : -1);
+    for (int c = wlo + lane; c <= whi; c += 32) {
+      const uint32_t m = bitmap[c];
+      if (m != 0u) {
+        base[c] += __popc(m);
+        bitmap[c] = 0u;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// The staged pairs out to their lists: one warp per column, consecutive
+// entries per lane.
+__device__ __forceinline__ void copy_out_staged(int extent, const int32_t* col_count,
+                                                const int32_t* col_start,
+                                                const int64_t* col_dst, const uint32_t* stage,
+                                                int64_t capacity, uint32_t* __restrict__ out) {
+  const int w = warp_id(), lane = lane_id();
+  for (int c = w; c < extent; c += kWarps) {
+    const int n = col_count[c], src = col_start[c];
+    const int64_t dst = col_dst[c];  // >= 0: offsets and bases are counts
+    for (int i = lane; i < n; i += 32)
+      if (dst + i < capacity) out[dst + i] = stage[src + i];
+  }
+}
+
+// Shared memory of an expansion over `extent` columns: [kWarps][extent]
+// counts then bases, the same shape of bitmaps, per column stage start, pair
+// count and list position, then the stage.
+struct ExpandSmem {
+  int32_t* cnt;
+  uint32_t* bitmap;
+  int32_t* col_start;
+  int32_t* col_count;
+  int64_t* col_dst;
+  uint32_t* stage;
+};
+
+__device__ __forceinline__ ExpandSmem expand_smem(int32_t* s_mem, int max_extent) {
+  ExpandSmem e;
+  e.cnt = s_mem;
+  e.bitmap = reinterpret_cast<uint32_t*>(s_mem + kWarps * max_extent);
+  e.col_start = s_mem + 2 * kWarps * max_extent;
+  e.col_count = e.col_start + max_extent;
+  // at byte 72 * max_extent of the 16-byte aligned block: 8-byte aligned
+  e.col_dst = reinterpret_cast<int64_t*>(e.col_count + max_extent);
+  e.stage = reinterpret_cast<uint32_t*>(e.col_dst + max_extent);
+  return e;
+}
+
 // Writes each chunk's records into its row's tile lists, in record (depth)
 // order: 32 records at a time per warp, a per-column bitmap giving each pair
 // its place among the lanes. The chunk's pairs are staged in shared memory
@@ -321,121 +389,146 @@ __global__ void __launch_bounds__(kWarps * 32)
                    const int32_t* __restrict__ chunk_base,
                    const int64_t* __restrict__ tile_offsets, int64_t capacity,
                    uint32_t* __restrict__ tile_slots) {
-  // [kWarps][max_tiles_x] counts then bases, the same shape of bitmaps,
-  // per column: stage start, pair count and list position; then the stage
   extern __shared__ __align__(16) int32_t s_mem[];
   __shared__ int s_warp[kWarps];
   if ((int)blockIdx.x >= n_chunks[0]) return;
   const int4 ch = chunks[blockIdx.x];
   const ViewDesc& vd = views[view_of_row(views, n_views, ch.x)];
   const int tiles_x = vd.tiles_x;
-  const int w = warp_id(), lane = lane_id();
-  int32_t* s_cnt = s_mem;
-  uint32_t* bitmap_all = reinterpret_cast<uint32_t*>(s_mem + kWarps * max_tiles_x);
-  int32_t* col_start = s_mem + 2 * kWarps * max_tiles_x;
-  int32_t* col_count = col_start + max_tiles_x;
-  // at byte 72 * max_tiles_x of the 16-byte aligned block: 8-byte aligned
-  int64_t* col_dst = reinterpret_cast<int64_t*>(col_count + max_tiles_x);
-  uint32_t* stage = reinterpret_cast<uint32_t*>(col_dst + max_tiles_x);
+  const int w = warp_id();
+  const ExpandSmem e = expand_smem(s_mem, max_tiles_x);
   for (int i = threadIdx.x; i < kWarps * tiles_x; i += blockDim.x) {
-    s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
-    bitmap_all[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0u;
+    e.cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
+    e.bitmap[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0u;
   }
   __syncthreads();
   uint32_t slot[kPerLane], xr[kPerLane];
-  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, s_cnt, slot, xr);
+  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, e.cnt, slot, xr);
   __syncthreads();
-  // per-column totals, then their exclusive scan: each column's stage start
-  const int per = (tiles_x + blockDim.x - 1) / blockDim.x;
-  const int c_begin = min(tiles_x, (int)threadIdx.x * per);
-  const int c_end = min(tiles_x, c_begin + per);
-  int mine = 0;
-  for (int c = c_begin; c < c_end; ++c) {
-    int t = 0;
-#pragma unroll
-    for (int k = 0; k < kWarps; ++k) t += s_cnt[k * max_tiles_x + c];
-    col_count[c] = t;
-    mine += t;
-  }
-  int total = 0;
-  int run_start = block_exclusive_scan(mine, s_warp, &total);
-  const bool staged = total <= kStage;  // block-uniform
   const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)(ch.x - vd.row_offset) * tiles_x;
-  for (int c = c_begin; c < c_end; ++c) {
-    col_start[c] = run_start;
-    col_dst[c] = tile_offsets[tile0 + c] + chunk_base[(int64_t)blockIdx.x * max_tiles_x + c];
-    // per warp, where its pairs of this column begin among the chunk's pairs
-    int run = run_start;
-#pragma unroll
-    for (int k = 0; k < kWarps; ++k) {
-      const int t = s_cnt[k * max_tiles_x + c];
-      s_cnt[k * max_tiles_x + c] = run;
-      run += t;
-    }
-    run_start += col_count[c];
-  }
-  __syncthreads();
-  int32_t* base = s_cnt + w * max_tiles_x;
-  uint32_t* bitmap = bitmap_all + w * max_tiles_x;
-  const unsigned lt = lanemask_lt();
-#pragma unroll
-  for (int k = 0; k < kPerLane; ++k) {
-    const int x0 = xr[k] & 0xFFFF, x1 = xr[k] >> 16;
-    for (int c = x0; c <= x1; ++c) atomicOr(&bitmap[c], 1u << lane);
-    __syncwarp();
-    for (int c = x0; c <= x1; ++c) {
-      const int pos = base[c] + __popc(bitmap[c] & lt);  // among the chunk's pairs
-      if (staged) {
-        stage[pos] = slot[k];
-      } else {
-        const int64_t dst = col_dst[c] + (pos - col_start[c]);
-        if (dst < capacity) tile_slots[dst] = slot[k];
-      }
-    }
-    __syncwarp();
-    const int lo = __reduce_min_sync(kFull, x1 >= x0 ? x0 : (1 << 30));
-    const int hi = __reduce_max_sync(kFull, x1 >= x0 ? x1 : -1);
-    for (int c = lo + lane; c <= hi; c += 32) {
-      const uint32_t m = bitmap[c];
-      if (m != 0u) {
-        base[c] += __popc(m);
-        bitmap[c] = 0u;
-      }
-    }
-    __syncwarp();
-  }
+  const bool staged = chunk_layout(
+      e.cnt, max_tiles_x, tiles_x, kStage, s_warp, e.col_count, e.col_start, e.col_dst,
+      [&](int c) {
+        return tile_offsets[tile0 + c] + chunk_base[(int64_t)blockIdx.x * max_tiles_x + c];
+      });
+  warp_range_expand(xr, slot, e.cnt + w * max_tiles_x, e.bitmap + w * max_tiles_x, staged,
+                    e.stage, e.col_start, e.col_dst, capacity, tile_slots);
   if (!staged) return;
   __syncthreads();
-  // copy out: one warp per column, consecutive entries per lane
-  for (int c = w; c < tiles_x; c += kWarps) {
-    const int n = col_count[c], src = col_start[c];
-    const int64_t dst = col_dst[c];  // >= 0: offsets and bases are counts
-    for (int i = lane; i < n; i += 32)
-      if (dst + i < capacity) tile_slots[dst + i] = stage[src + i];
+  copy_out_staged(tiles_x, e.col_count, e.col_start, e.col_dst, e.stage, capacity, tile_slots);
+}
+
+// ------------------------------------------------------------ tile-row records
+//
+// The records -- one (tile row, slot) per row a visible splat covers -- are
+// wanted grouped by row (rows of every view one after another) and, within a
+// row, in depth order. Each view's depth-sorted slots are cut into chunks of
+// kSlotChunk; a chunk counts, per tile row of its view, the splats covering
+// it; an exclusive scan of those counts in (row, chunk) order gives every
+// chunk its base in every row; the chunk then writes its records there with
+// the same bitmap ranking and staging as the tile lists (rows for columns).
+// This is the stable counting sort of the records by row, with no sort pass.
+constexpr int kSlotChunk = 512;
+constexpr int kSlotPerLane = kSlotChunk / (kWarps * 32);  // slots per lane per chunk
+
+// Lane slots of a chunk starting at `begin` of the depth-sorted slots, and
+// their tile-row ranges (empty for a culled slot).
+__device__ __forceinline__ void chunk_slot_rows(const uint32_t* __restrict__ sorted_slots,
+                                                const int32_t* __restrict__ tile_count,
+                                                const uint2* __restrict__ rect, int64_t begin,
+                                                uint32_t (&slot)[kSlotPerLane],
+                                                uint32_t (&yr)[kSlotPerLane]) {
+  const int w = warp_id(), lane = lane_id();
+#pragma unroll
+  for (int k = 0; k < kSlotPerLane; ++k) {
+    const int64_t i = begin + w * (kSlotChunk / kWarps) + k * 32 + lane;
+    slot[k] = sorted_slots[i];
+    yr[k] = 1u;  // y0 = 1 > y1 = 0: no rows
   }
+#pragma unroll
+  for (int k = 0; k < kSlotPerLane; ++k)
+    if (tile_count[slot[k]] > 0) yr[k] = rect[slot[k]].y;
+}
+
+// counts[(row_offset + y) * cpv + c]: splats of chunk c of view v (block
+// v * cpv + c) covering tile row y of the view.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_slot_row_counts(const uint32_t* __restrict__ sorted_slots,
+                      const int32_t* __restrict__ tile_count, const uint2* __restrict__ rect,
+                      const ViewDesc* __restrict__ views, int64_t slot_stride, int cpv,
+                      int max_tiles_y, int32_t* __restrict__ counts) {
+  extern __shared__ int32_t s_cnt[];  // [kWarps][max_tiles_y]
+  const int v = blockIdx.x / cpv, c = blockIdx.x % cpv;
+  const ViewDesc& vd = views[v];
+  const int tiles_y = vd.tiles_y;
+  for (int i = threadIdx.x; i < kWarps * tiles_y; i += blockDim.x)
+    s_cnt[(i / tiles_y) * max_tiles_y + (i % tiles_y)] = 0;
+  __syncthreads();
+  uint32_t slot[kSlotPerLane], yr[kSlotPerLane];
+  chunk_slot_rows(sorted_slots, tile_count, rect, (int64_t)v * slot_stride + (int64_t)c * kSlotChunk,
+                  slot, yr);
+  warp_range_counts(yr, tiles_y, s_cnt + warp_id() * max_tiles_y);
+  __syncthreads();
+  for (int y = threadIdx.x; y < tiles_y; y += blockDim.x) {
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) total += s_cnt[k * max_tiles_y + y];
+    counts[(int64_t)(vd.row_offset + y) * cpv + c] = total;
+  }
+}
+
+// The chunk's records at offsets[(row_offset + y) * cpv + c] onwards in each
+// row y, in slot order; nothing at or past `capacity`.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_slot_row_expand(const uint32_t* __restrict__ sorted_slots,
+                      const int32_t* __restrict__ tile_count, const uint2* __restrict__ rect,
+                      const ViewDesc* __restrict__ views, int64_t slot_stride, int cpv,
+                      int max_tiles_y, const int64_t* __restrict__ offsets, int64_t capacity,
+                      uint32_t* __restrict__ rec_slots) {
+  extern __shared__ __align__(16) int32_t s_mem[];
+  __shared__ int s_warp[kWarps];
+  const int v = blockIdx.x / cpv, c = blockIdx.x % cpv;
+  const ViewDesc& vd = views[v];
+  const int tiles_y = vd.tiles_y;
+  const int w = warp_id();
+  const ExpandSmem e = expand_smem(s_mem, max_tiles_y);
+  for (int i = threadIdx.x; i < kWarps * tiles_y; i += blockDim.x) {
+    e.cnt[(i / tiles_y) * max_tiles_y + (i % tiles_y)] = 0;
+    e.bitmap[(i / tiles_y) * max_tiles_y + (i % tiles_y)] = 0u;
+  }
+  __syncthreads();
+  uint32_t slot[kSlotPerLane], yr[kSlotPerLane];
+  chunk_slot_rows(sorted_slots, tile_count, rect, (int64_t)v * slot_stride + (int64_t)c * kSlotChunk,
+                  slot, yr);
+  warp_range_counts(yr, tiles_y, e.cnt + w * max_tiles_y);
+  __syncthreads();
+  const bool staged = chunk_layout(
+      e.cnt, max_tiles_y, tiles_y, kStage, s_warp, e.col_count, e.col_start, e.col_dst,
+      [&](int y) { return offsets[(int64_t)(vd.row_offset + y) * cpv + c]; });
+  warp_range_expand(yr, slot, e.cnt + w * max_tiles_y, e.bitmap + w * max_tiles_y, staged,
+                    e.stage, e.col_start, e.col_dst, capacity, rec_slots);
+  if (!staged) return;
+  __syncthreads();
+  copy_out_staged(tiles_y, e.col_count, e.col_start, e.col_dst, e.stage, capacity, rec_slots);
+}
+
+// row_ranges[r] = [offsets[r * cpv], offsets[(r + 1) * cpv]) (the total for the
+// last row), clamped to the capacity; records past it raise the overflow flag.
+__global__ void k_row_ranges_from_chunks(const int64_t* __restrict__ offsets, int total_rows,
+                                         int cpv, const int64_t* __restrict__ total,
+                                         int64_t capacity, int2* __restrict__ row_ranges,
+                                         int32_t* __restrict__ overflow) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= total_rows) return;
+  int64_t b = offsets[(int64_t)r * cpv];
+  int64_t e = r + 1 < total_rows ? offsets[(int64_t)(r + 1) * cpv] : *total;
+  if (e > capacity) atomicExch(overflow, 1);
+  b = b < capacity ? b : capacity;
+  e = e < capacity ? e : capacity;
+  row_ranges[r] = make_int2((int)b, (int)e);
 }
 
 // ------------------------------------------------------------------ host
-
-void launch_gather_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
-                              const uint2* rect, int64_t n, int32_t* counts,
-                              cudaStream_t stream) {
-  if (n <= 0) return;
-  count_launch();
-  k_gather_row_counts<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(sorted_slots, tile_count,
-                                                                       rect, n, counts);
-}
-
-void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const int64_t* offsets,
-                      const uint2* rect, const ViewDesc* views, int64_t slot_stride, int64_t n,
-                      uint32_t* keys, uint32_t* vals, int64_t capacity, uint32_t sentinel_row,
-                      int32_t* overflow, cudaStream_t stream) {
-  if (n <= 0) return;
-  count_launch();
-  k_emit_rows<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
-      sorted_slots, counts, offsets, rect, views, slot_stride, n, keys, vals, capacity,
-      sentinel_row, overflow);
-}
 
 size_t chunk_counts_smem(int max_tiles_x) { return sizeof(int32_t) * kWarps * max_tiles_x; }
 size_t chunk_expand_smem(int max_tiles_x) {
@@ -443,11 +536,52 @@ size_t chunk_expand_smem(int max_tiles_x) {
          sizeof(int64_t) * (size_t)max_tiles_x;
 }
 
+size_t slot_row_counts_smem(int max_tiles_y) { return sizeof(int32_t) * kWarps * max_tiles_y; }
+
 void configure_bin_kernels() {
   cudaFuncSetAttribute(k_chunk_counts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)chunk_counts_smem(kMaxTilesX));
   cudaFuncSetAttribute(k_chunk_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)chunk_expand_smem(kMaxTilesX));
+  cudaFuncSetAttribute(k_slot_row_counts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)slot_row_counts_smem(kMaxTilesY));
+  cudaFuncSetAttribute(k_slot_row_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)chunk_expand_smem(kMaxTilesY));
+}
+
+int slot_chunks_per_view(int64_t slot_stride) { return (int)(slot_stride / kSlotChunk); }
+
+void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
+                            const uint2* rect, const ViewDesc* views, int n_views,
+                            int64_t slot_stride, int max_tiles_y, int32_t* counts,
+                            cudaStream_t stream) {
+  const int cpv = slot_chunks_per_view(slot_stride);
+  if (n_views <= 0 || cpv <= 0) return;
+  count_launch();
+  k_slot_row_counts<<<(unsigned)(n_views * cpv), kWarps * 32, slot_row_counts_smem(max_tiles_y),
+                      stream>>>(sorted_slots, tile_count, rect, views, slot_stride, cpv,
+                                max_tiles_y, counts);
+}
+
+void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
+                            const uint2* rect, const ViewDesc* views, int n_views,
+                            int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
+                            int64_t capacity, uint32_t* rec_slots, cudaStream_t stream) {
+  const int cpv = slot_chunks_per_view(slot_stride);
+  if (n_views <= 0 || cpv <= 0) return;
+  count_launch();
+  k_slot_row_expand<<<(unsigned)(n_views * cpv), kWarps * 32, chunk_expand_smem(max_tiles_y),
+                      stream>>>(sorted_slots, tile_count, rect, views, slot_stride, cpv,
+                                max_tiles_y, offsets, capacity, rec_slots);
+}
+
+void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int cpv,
+                                   const int64_t* total, int64_t capacity, int2* row_ranges,
+                                   int32_t* overflow, cudaStream_t stream) {
+  if (total_rows <= 0) return;
+  count_launch();
+  k_row_ranges_from_chunks<<<(unsigned)((total_rows + 255) / 256), 256, 0, stream>>>(
+      offsets, total_rows, cpv, total, capacity, row_ranges, overflow);
 }
 
 int64_t max_row_chunks(int64_t records, int total_rows) { return records / kChunk + total_rows + 1; }

@@ -57,21 +57,27 @@ int radix_sort_pairs(uint32_t*& keys, uint32_t*& vals, uint32_t*& keys_alt,
                      uint32_t* hist, uint32_t* hist_scanned, ScanScratch& scratch,
                      cudaStream_t stream, const int64_t* n_device = nullptr);
 void launch_iota(uint32_t* out, int64_t n, cudaStream_t stream);
-void launch_gather_counts(const uint32_t* sorted_slots, const int32_t* tile_count, int64_t n,
-                          int32_t* counts, cudaStream_t stream);
-// n is an upper bound when n_device (the device-side pair count) is given.
-void launch_tile_ranges(const uint32_t* keys, int64_t n, const int64_t* n_device,
-                        uint32_t n_tiles, int2* ranges, cudaStream_t stream);
 
 // bin.cu
 void configure_bin_kernels();  // once per device, outside graph capture
-void launch_gather_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
-                              const uint2* rect, int64_t n, int32_t* counts,
-                              cudaStream_t stream);
-void launch_emit_rows(const uint32_t* sorted_slots, const int32_t* counts, const int64_t* offsets,
-                      const uint2* rect, const ViewDesc* views, int64_t slot_stride, int64_t n,
-                      uint32_t* keys, uint32_t* vals, int64_t capacity, uint32_t sentinel_row,
-                      int32_t* overflow, cudaStream_t stream);
+// Tile-row records grouped by row, depth order within a row (bin.cu): per
+// (view, chunk of depth-sorted slots) the splats covering each tile row of the
+// view, counts[(row_offset + y) * cpv + c]; after their exclusive scan into
+// offsets, each chunk writes its records (slot ids) at its bases.
+int slot_chunks_per_view(int64_t slot_stride);
+void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
+                            const uint2* rect, const ViewDesc* views, int n_views,
+                            int64_t slot_stride, int max_tiles_y, int32_t* counts,
+                            cudaStream_t stream);
+void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
+                            const uint2* rect, const ViewDesc* views, int n_views,
+                            int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
+                            int64_t capacity, uint32_t* rec_slots, cudaStream_t stream);
+// Per-row record ranges from the chunk offsets, clamped to the capacity
+// (records past it raise the overflow flag).
+void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int cpv,
+                                   const int64_t* total, int64_t capacity, int2* row_ranges,
+                                   int32_t* overflow, cudaStream_t stream);
 // Upper bound on the number of row chunks for `records` records.
 int64_t max_row_chunks(int64_t records, int total_rows);
 // Chunk table, per-chunk column counts, per-chunk bases and tile lengths.

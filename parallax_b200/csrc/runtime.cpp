@@ -61,8 +61,8 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
     d.sh_degree = std::min(options.sh_degree, cloud_sh_degree);
     d.tiles_x = (d.cam.width + kTile - 1) / kTile;
     d.tiles_y = (d.cam.height + kTile - 1) / kTile;
-    if (d.tiles_x > kMaxTilesX || d.tiles_y > 0xFFFF)
-      throw Error(PXS_ERR_INVALID, "image too large (at most 2048 tiles across)");
+    if (d.tiles_x > kMaxTilesX || d.tiles_y > kMaxTilesY)
+      throw Error(PXS_ERR_INVALID, "image too large (at most 2048 tiles across and down)");
     d.tile_offset = tile_offset;
     d.row_offset = row_offset;
     d.loss_tile_offset = static_cast<int32_t>(loss_tile_offset);
@@ -75,6 +75,7 @@ ViewBatch make_batch(const pxs_camera* cameras, int n_views, const pxs_raster_op
     tile_offset += d.tiles_x * d.tiles_y;
     row_offset += d.tiles_y;
     b.max_tiles_x = std::max(b.max_tiles_x, d.tiles_x);
+    b.max_tiles_y = std::max(b.max_tiles_y, d.tiles_y);
     pixel_offset += static_cast<int64_t>(d.cam.width) * d.cam.height;
     b.max_width = std::max(b.max_width, d.cam.width);
     b.max_height = std::max(b.max_height, d.cam.height);
@@ -133,8 +134,10 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   sort_vals.reserve(slots);
   sort_keys_alt.reserve(slots);
   sort_vals_alt.reserve(slots);
-  counts.reserve(slots);
-  pair_offsets.reserve(slots);
+  const size_t row_chunks = static_cast<size_t>(std::max(batch.total_rows, 1)) *
+                            static_cast<size_t>(std::max(slot_chunks_per_view(slot_stride), 1));
+  row_chunk_counts.reserve(row_chunks);
+  row_chunk_offsets.reserve(row_chunks);
   d_total_pairs.reserve(1);
   screen.reserve(slots);
   overflow.reserve(1);
@@ -177,20 +180,11 @@ void Frame::reserve_pairs(int64_t capacity) {
 
 void Frame::reserve_records(int64_t capacity) {
   if (capacity > INT32_MAX) throw Error(PXS_ERR_CAPACITY, "more than 2^31 tile-row records");
-  if (capacity <= record_capacity && rec_keys.get() != nullptr) return;
+  if (capacity <= record_capacity && rec_vals.get() != nullptr) return;
   const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
-  rec_keys.reserve(cap);
   rec_vals.reserve(cap);
-  rec_keys_alt.reserve(cap);
-  rec_vals_alt.reserve(cap);
   record_capacity = static_cast<int64_t>(cap);
   ensure_chunks();
-  const size_t rec_hist = radix_hist_entries(record_capacity, 0, 9);
-  if (hist.capacity() < rec_hist) {
-    hist.reserve(rec_hist);
-    hist_scanned.reserve(rec_hist);
-  }
-  ensure_scan_scratch(static_cast<int64_t>(hist.capacity()));
 }
 
 void Frame::ensure_chunks() {
@@ -233,10 +227,15 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   radix_sort_pairs(k, v, ka, va, slots, slot_stride, 32, hist.get(), hist_scanned.get(), scan_,
                    stream);
   sorted_slots = v;
-  // 2. one record per covered tile row, in that order
-  launch_gather_row_counts(v, tile_count.get(), rect.get(), slots, counts.get(), stream);
-  exclusive_scan_i32_to_i64(counts.get(), pair_offsets.get(), slots, d_total_records.get(),
-                            scan_, stream);
+  // 2. one record per covered tile row, grouped by row and near to far within
+  //    a row: per (view, slot chunk) row counts, their scan in (row, chunk)
+  //    order, then each chunk writes its records at its bases
+  const int cpv = slot_chunks_per_view(slot_stride);
+  const int64_t n_row_chunks = static_cast<int64_t>(batch.total_rows) * cpv;
+  launch_slot_row_counts(v, tile_count.get(), rect.get(), d_views.get(), V, slot_stride,
+                         batch.max_tiles_y, row_chunk_counts.get(), stream);
+  exclusive_scan_i32_to_i64(row_chunk_counts.get(), row_chunk_offsets.get(), n_row_chunks,
+                            d_total_records.get(), scan_, stream);
   PXS_CUDA(cudaGetLastError());
   if (host_sync) {
     PXS_CUDA(cudaMemcpyAsync(&last_record_count, d_total_records.get(), sizeof(int64_t),
@@ -244,24 +243,17 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
     PXS_CUDA(cudaStreamSynchronize(stream));
     if (last_record_count > record_capacity)
       reserve_records(last_record_count + last_record_count / 8 + 1024);
-  } else if (rec_keys.get() == nullptr || tile_slots.get() == nullptr) {
+  } else if (rec_vals.get() == nullptr || tile_slots.get() == nullptr) {
     throw Error(PXS_ERR_INVALID, "pair buffers must be reserved before an unsynchronised bin");
   }
   PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
-  const uint32_t n_rows = static_cast<uint32_t>(batch.total_rows);
-  launch_emit_rows(v, counts.get(), pair_offsets.get(), rect.get(), d_views.get(), slot_stride,
-                   slots, rec_keys.get(), rec_vals.get(), record_capacity, n_rows,
-                   overflow.get(), stream);
-  // 3. records grouped by row, depth order kept (one spare key: the sentinel)
-  uint32_t *rk = rec_keys.get(), *rv = rec_vals.get();
-  uint32_t *rka = rec_keys_alt.get(), *rva = rec_vals_alt.get();
-  const int64_t n_rec = host_sync ? last_record_count : record_capacity;
-  const int64_t* n_dev = host_sync ? nullptr : d_total_records.get();
-  radix_sort_pairs(rk, rv, rka, rva, n_rec, 0, bits_for(int64_t(batch.total_rows) + 1),
-                   hist.get(), hist_scanned.get(), scan_, stream, n_dev);
-  PXS_CUDA(cudaMemsetAsync(row_ranges.get(), 0, sizeof(int2) * std::max(batch.total_rows, 1),
-                           stream));
-  launch_tile_ranges(rk, n_rec, n_dev, n_rows, row_ranges.get(), stream);
+  launch_slot_row_expand(v, tile_count.get(), rect.get(), d_views.get(), V, slot_stride,
+                         batch.max_tiles_y, row_chunk_offsets.get(), record_capacity,
+                         rec_vals.get(), stream);
+  launch_row_ranges_from_chunks(row_chunk_offsets.get(), batch.total_rows, cpv,
+                                d_total_records.get(), record_capacity, row_ranges.get(),
+                                overflow.get(), stream);
+  const uint32_t* rv = rec_vals.get();
   // 4. tile lengths from chunked rows, their offsets, then the lists themselves
   ensure_chunks();
   launch_tile_lists(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,

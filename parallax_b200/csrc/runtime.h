@@ -92,7 +92,7 @@ struct ViewBatch {
   int64_t total_pixels = 0;
   int total_tiles = 0;
   int total_rows = 0;       // tile rows over all views
-  int max_tiles_x = 0;
+  int max_tiles_x = 0, max_tiles_y = 0;
   int max_width = 0, max_height = 0;
   // the views carry their own gaussian ranges (several scenes); otherwise
   // Frame::prepare gives every view the whole cloud
@@ -155,9 +155,10 @@ class Frame {
   DeviceArray<uint2> rect;
   DeviceArray<int32_t> tile_count;
   DeviceArray<uint32_t> sort_keys, sort_vals, sort_keys_alt, sort_vals_alt;
-  DeviceArray<int32_t> counts;
-  DeviceArray<int64_t> pair_offsets, d_total_pairs, d_total_records;
-  DeviceArray<uint32_t> rec_keys, rec_vals, rec_keys_alt, rec_vals_alt;  // tile-row records
+  // per (tile row, chunk of depth-sorted slots): records and their offsets
+  DeviceArray<int32_t> row_chunk_counts;
+  DeviceArray<int64_t> row_chunk_offsets, d_total_pairs, d_total_records;
+  DeviceArray<uint32_t> rec_vals;  // tile-row records (slot ids) by row, near to far
   DeviceArray<int2> row_ranges;
   DeviceArray<int32_t> tile_counts, chunk_counts, chunk_base, n_chunks;
   DeviceArray<int4> chunks;

@@ -250,44 +250,6 @@ __global__ void k_iota(uint32_t* __restrict__ out, int64_t n) {
   if (i < n) out[i] = (uint32_t)i;
 }
 
-// Tiles touched by the i-th nearest slot of each view.
-__global__ void k_gather_counts(const uint32_t* __restrict__ sorted_slots,
-                                const int32_t* __restrict__ tile_count, int64_t n,
-                                int32_t* __restrict__ counts) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) counts[i] = tile_count[sorted_slots[i]];
-}
-
-__global__ void __launch_bounds__(256)
-    k_tile_ranges(const uint32_t* __restrict__ keys, int64_t n_max,
-                  const int64_t* __restrict__ n_device, uint32_t n_tiles,
-                  int2* __restrict__ ranges) {
-  const int64_t n = n_device != nullptr ? min(*n_device, n_max) : n_max;
-  const int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (i0 >= n) return;
-  uint32_t k[6];  // keys[i0-1 .. i0+4]
-  k[0] = i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu;
-  if (i0 + 4 <= n) {
-    const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
-    k[1] = q.x;
-    k[2] = q.y;
-    k[3] = q.z;
-    k[4] = q.w;
-  } else {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) k[1 + j] = i0 + j < n ? keys[i0 + j] : 0xFFFFFFFFu;
-  }
-  k[5] = i0 + 4 < n ? keys[i0 + 4] : 0xFFFFFFFFu;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int64_t i = i0 + j;
-    if (i >= n) break;
-    const uint32_t key = k[1 + j];
-    if (key >= n_tiles) continue;  // overflow sentinels
-    if (i == 0 || k[j] != key) ranges[key].x = (int)i;
-    if (i == n - 1 || k[2 + j] != key) ranges[key].y = (int)(i + 1);
-  }
-}
 
 }  // namespace
 
@@ -391,24 +353,6 @@ void launch_iota(uint32_t* out, int64_t n, cudaStream_t stream) {
   if (n > 0) {
     count_launch();
     k_iota<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(out, n);
-  }
-}
-
-void launch_gather_counts(const uint32_t* sorted_slots, const int32_t* tile_count, int64_t n,
-                          int32_t* counts, cudaStream_t stream) {
-  if (n > 0) {
-    count_launch();
-    k_gather_counts<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(sorted_slots, tile_count, n,
-                                                                     counts);
-  }
-}
-
-void launch_tile_ranges(const uint32_t* keys, int64_t n, const int64_t* n_device,
-                        uint32_t n_tiles, int2* ranges, cudaStream_t stream) {
-  if (n > 0) {
-    count_launch();
-    k_tile_ranges<<<(unsigned)((n + 1023) / 1024), 256, 0, stream>>>(keys, n, n_device, n_tiles,
-                                                                     ranges);
   }
 }
 
