@@ -14,15 +14,23 @@
 namespace pxs {
 
 
+constexpr int kProjectThreads = 256;
+
 // One thread per slot index i, looping over the views of the batch: view v's
 // slot i holds gaussian gauss_offset + i of that view's range. Views of one
 // cloud share the gaussian, so its parameters are read once; a batch of
 // several scenes reads each scene's gaussian when the scene changes
-// (projectSplats, SplatRaster.cpp:201-258).
-__global__ void __launch_bounds__(256)
-    k_project(const float* __restrict__ params, int N, int S, int64_t slot_stride,
+// (projectSplats, SplatRaster.cpp:201-258). The gaussian's S SH-rest
+// coefficients per channel are read together into this thread's column of
+// shared memory and serve every view.
+template <int S>
+__global__ void __launch_bounds__(kProjectThreads)
+    k_project(const float* __restrict__ params, int N, int64_t slot_stride,
               const ViewDesc* __restrict__ views, int n_views, ProjectedSoA out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int kRest = 3 * S > 0 ? 3 * S : 1;
+  __shared__ float s_sh[kRest][kProjectThreads];
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + t;
   if (i >= slot_stride) return;
   GaussianState st;
   int g = -1;  // the gaussian whose state is loaded
@@ -38,6 +46,13 @@ __global__ void __launch_bounds__(256)
     }
     if (vd.gauss_offset + i != g) {
       g = vd.gauss_offset + i;
+      if constexpr (S > 0) {
+        float sh[3 * S];
+#pragma unroll
+        for (int j = 0; j < 3 * S; ++j) sh[j] = params[(int64_t)(PXS_C_SH_REST + j) * N + g];
+#pragma unroll
+        for (int j = 0; j < 3 * S; ++j) s_sh[j][t] = sh[j];
+      }
       load_state(params, N, g, st);
       dc0 = params[(int64_t)(PXS_C_DC + 0) * N + g];
       dc1 = params[(int64_t)(PXS_C_DC + 1) * N + g];
@@ -109,8 +124,9 @@ __global__ void __launch_bounds__(256)
     const int usable = count < S ? count : S;
     for (int c = 0; c < 3; ++c) {
       float sum = 0.f;
-      for (int k = 0; k < usable; ++k)
-        sum += basis[k] * params[(int64_t)(PXS_C_SH_REST + c * S + k) * N + g];
+#pragma unroll
+      for (int k = 0; k < S; ++k)
+        if (k < usable) sum += basis[k] * s_sh[c * S + k][t];
       color[c] += sum;
     }
     uint32_t flags = 0;
@@ -143,11 +159,23 @@ __global__ void __launch_bounds__(256)
 void launch_project(const float* params, int N, int S, int64_t slot_stride,
                     const ViewDesc* views, int n_views, const ProjectedSoA& out,
                     cudaStream_t stream) {
-  const int threads = 256;
+  const int threads = kProjectThreads;
   const int blocks = (int)((slot_stride + threads - 1) / threads);
-  if (blocks > 0) {
-    count_launch();
-    k_project<<<blocks, threads, 0, stream>>>(params, N, S, slot_stride, views, n_views, out);
+  if (blocks <= 0) return;
+  count_launch();
+  switch (S) {
+    case 0:
+      k_project<0><<<blocks, threads, 0, stream>>>(params, N, slot_stride, views, n_views, out);
+      break;
+    case 3:
+      k_project<3><<<blocks, threads, 0, stream>>>(params, N, slot_stride, views, n_views, out);
+      break;
+    case 8:
+      k_project<8><<<blocks, threads, 0, stream>>>(params, N, slot_stride, views, n_views, out);
+      break;
+    default:
+      k_project<15><<<blocks, threads, 0, stream>>>(params, N, slot_stride, views, n_views, out);
+      break;
   }
 }
 

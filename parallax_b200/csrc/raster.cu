@@ -161,6 +161,8 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
   __shared__ float4 s_col[kBatch];  // r, g, b, power floor
   __shared__ uint32_t s_mask[kBatch];
   __shared__ uint8_t s_took[TileGeom<2>::kWarps][kBatch];  // warp w = 8x8 block w
+  __shared__ uint8_t s_list[TileGeom<2>::kWarps][kBatch];  // a warp's entries of the batch
+  static_assert(kBatch <= 256, "batch indices are bytes");
   const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
   const int warp = threadIdx.x >> 5;
   const ViewDesc& vd = views[info.view];
@@ -206,45 +208,69 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
       s_mask[i] = warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
     }
     __syncthreads();
-    if (!(done0 && done1)) {
-      for (int j = 0; j < n; ++j) {
-        if (kCount) evaluated += (done0 ? 0 : 1) + (done1 ? 0 : 1);
-        if (!((s_mask[j] >> warp) & 1u)) continue;  // cannot reach this warp's pixels
-        const float2 m = s_xy[j];
-        const float4 co = s_co[j];
-        const float floor = s_col[j].w;
-        const float dx = fx - m.x;
-        const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
-        const float2 power = splat_power2(co, dx, dy);
-        const bool in0 = !done0 && !(power.x > 0.f || power.x < floor);
-        const bool in1 = !done1 && !(power.y > 0.f || power.y < floor);
-        if (!(in0 || in1)) continue;
-        float a0 = in0 ? co.w * expf(power.x) : 0.f;
-        float a1 = in1 ? co.w * expf(power.y) : 0.f;
-        a0 = a0 < kMaxAlpha ? a0 : kMaxAlpha;
-        a1 = a1 < kMaxAlpha ? a1 : kMaxAlpha;
-        const bool c0 = in0 && !(a0 < min_alpha);
-        const bool c1 = in1 && !(a1 < min_alpha);
-        if (!(c0 || c1)) continue;
-        if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
-        if (kBits) s_took[warp][j] = 1;  // same value from every lane
-        const float4 c = s_col[j];
-        const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
-        acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
-        acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
-        acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
-        if (c0) {
-          T.x *= 1.f - a0;
-          last0 = base + j + 1;
-          if (T.x < cutoff) done0 = true;
-        }
-        if (c1) {
-          T.y *= 1.f - a1;
-          last1 = base + j + 1;
-          if (T.y < cutoff) done1 = true;
-        }
-        if (done0 && done1) break;
+    // entry j for this warp's pixels; returns whether both are done
+    auto visit = [&](int j) -> bool {
+      const float2 m = s_xy[j];
+      const float4 co = s_co[j];
+      const float floor = s_col[j].w;
+      const float dx = fx - m.x;
+      const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
+      const float2 power = splat_power2(co, dx, dy);
+      const bool in0 = !done0 && !(power.x > 0.f || power.x < floor);
+      const bool in1 = !done1 && !(power.y > 0.f || power.y < floor);
+      if (!(in0 || in1)) return false;
+      float a0 = in0 ? co.w * expf(power.x) : 0.f;
+      float a1 = in1 ? co.w * expf(power.y) : 0.f;
+      a0 = a0 < kMaxAlpha ? a0 : kMaxAlpha;
+      a1 = a1 < kMaxAlpha ? a1 : kMaxAlpha;
+      const bool c0 = in0 && !(a0 < min_alpha);
+      const bool c1 = in1 && !(a1 < min_alpha);
+      if (!(c0 || c1)) return false;
+      if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
+      if (kBits) s_took[warp][j] = 1;  // same value from every lane
+      const float4 c = s_col[j];
+      const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
+      acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
+      acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
+      acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
+      if (c0) {
+        T.x *= 1.f - a0;
+        last0 = base + j + 1;
+        if (T.x < cutoff) done0 = true;
       }
+      if (c1) {
+        T.y *= 1.f - a1;
+        last1 = base + j + 1;
+        if (T.y < cutoff) done1 = true;
+      }
+      return done0 && done1;
+    };
+    if (kCount) {
+      if (!(done0 && done1)) {
+        // every entry counts as evaluated for each pixel not yet done
+        for (int j = 0; j < n; ++j) {
+          evaluated += (done0 ? 0 : 1) + (done1 ? 0 : 1);
+          if (!((s_mask[j] >> warp) & 1u)) continue;  // cannot reach this warp's pixels
+          if (visit(j)) break;
+        }
+      }
+    } else {
+      // the entries whose footprint can reach this warp's block, ascending;
+      // built by the whole warp (every lane is here, after the barrier above)
+      // before each lane walks it for its own pixels
+      const int lane = threadIdx.x & 31;
+      int n_mine = 0;
+      for (int j0 = 0; j0 < n; j0 += 32) {
+        const int jj = j0 + lane;
+        const bool mine = jj < n && ((s_mask[jj] >> warp) & 1u);
+        const unsigned b = __ballot_sync(0xffffffffu, mine);
+        if (mine) s_list[warp][n_mine + __popc(b & lanemask_lt())] = (uint8_t)jj;
+        n_mine += __popc(b);
+      }
+      __syncwarp();
+      if (!(done0 && done1))
+        for (int q = 0; q < n_mine; ++q)
+          if (visit(s_list[warp][q])) break;
     }
     prev_base = base;
     prev_n = n;

@@ -254,7 +254,9 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
   __shared__ float4 s_col[kBatch];  // r, g, b, power floor
   __shared__ uint32_t s_mask[kBatch];
   __shared__ float s_acc[kBatch][12];
+  __shared__ uint8_t s_list[TileGeom<2>::kWarps][kBatch];  // a warp's entries of the batch
   __shared__ int s_hi;
+  static_assert(kBatch <= 256, "batch indices are bytes");
   const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha;
@@ -319,8 +321,18 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
     }
     __syncthreads();
     const int j_top = min(n, warp_hi - batch_start) - 1;  // warp-uniform
-    for (int j = j_top; j >= 0; --j) {
-      if (!((s_mask[j] >> warp) & 1u)) continue;  // no pixel of this warp takes it
+    // the entries some pixel of this warp takes (or can reach), ascending
+    int n_mine = 0;
+    for (int j0 = 0; j0 <= j_top; j0 += 32) {
+      const int jj = j0 + lane;
+      const bool mine = jj <= j_top && ((s_mask[jj] >> warp) & 1u);
+      const unsigned b = __ballot_sync(kFull, mine);
+      if (mine) s_list[warp][n_mine + __popc(b & lanemask_lt())] = (uint8_t)jj;
+      n_mine += __popc(b);
+    }
+    __syncwarp();
+    for (int q = n_mine - 1; q >= 0; --q) {  // back to front
+      const int j = s_list[warp][q];
       const int e = batch_start + j;
       const float2 m = s_xy[j];
       const float4 co = s_co[j];

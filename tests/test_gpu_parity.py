@@ -482,6 +482,46 @@ def test_batched_and_graph_steps_match_the_plain_multi_view_step():
     assert np.abs(p0 - p1).max() <= 1e-4 and np.abs(p1 - p2).max() <= 1e-4
 
 
+def test_a_graph_step_whose_tile_lists_overflow_is_redone():
+    """The unsynchronised step runs with the pair and record capacities learned
+    on its first batch (with headroom). A later batch with many more tile pairs
+    -- cameras much closer -- overflows them: the step is discarded, the
+    buffers grown and the step redone, matching the host-synchronised plain
+    step as closely as the batched and plain forms match each other."""
+    params, rest = O.random_cloud(61, 20000, 3, log_scale_mean=-2.5)
+    truth, _ = O.random_cloud(62, 20000, 3, log_scale_mean=-2.5)
+    far = O.orbit_views(2, 160, 120, radius=9.0, seed=5)
+    near = O.orbit_views(2, 160, 120, radius=2.2, seed=6)
+    views = far + near
+    images = [px.render_splats(px.GaussianCloud(truth, 3, rest), v.camera(),
+                               RasterOptions(sh_degree=3))[0] for v in views]
+    cfg = TrainConfig(iterations=100, sh_degree=3, sh_increase_interval=0,
+                      densify_from_iteration=1000, densify_until_iteration=1000)
+    pairs = [(v.camera(), im) for v, im in zip(views, images)]
+    lib = px.lib()
+    results, step_pairs = [], []
+    for mode in ("plain", "graph"):
+        t = px.SplatTrainer(px.GaussianCloud(params, 3, rest), pairs, cfg)
+        losses = []
+        for sel in ([0, 1], [2, 3]):
+            if mode == "plain":
+                losses.append(t.step_views(2, sel))
+            else:
+                losses.append(t.step_batch(2, sel, graph=True))
+                k, launches = ct.c_int64(), ct.c_int64()
+                t._check(lib.pxs_trainer_step_info(t.handle, ct.byref(k), ct.byref(launches)))
+                step_pairs.append(k.value)
+        results.append((losses, t.cloud_params()))
+        t.close()
+    k_far, k_near = step_pairs
+    print(f"tile pairs: far step {k_far}, near step {k_near}")
+    # the capacity learned on the far step is 1.5 K + 65536 pairs
+    assert k_near > 1.5 * k_far + 65536, "the near step did not overflow"
+    (l0, p0), (l1, p1) = results
+    assert np.allclose(l0, l1, rtol=1e-5)
+    assert np.abs(p0 - p1).max() <= 1e-4
+
+
 def test_train_splats_on_gpu_writes_back_a_finished_cloud():
     views, images = blob_scene(4, 16)
     start, _ = O.rough_start(10)
