@@ -21,7 +21,7 @@ __device__ __forceinline__ float adam_delta(float& m, float& v, float g, float l
   return -lr * m_hat / (sqrtf(v_hat) + eps);
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_adam(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m,
            float* __restrict__ v, int N, int S, const StepScalars* __restrict__ scalars,
            int zero_grads, float* __restrict__ screen_gradient,
