@@ -27,6 +27,16 @@ constexpr int kDirectLanes = 2;
 
 // Sums v[0..9] over the warp. Returns, in ten of the even lanes, one complete
 // sum; *idx is the index of that value, or -1 in the other lanes.
+// |d(mean)| for the densification statistic (the sum of per-pixel gradient
+// norms compared against a threshold): the hardware square root
+// approximation (relative error about 2^-22) instead of the correctly
+// rounded one, which costs several instructions more per pixel.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ float warp_reduce10(const float (&v)[10], int lane, int* idx) {
   const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
   float w[6];
@@ -188,7 +198,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
                 const float dm1 = dL_dweight * (-gy * co.z - gx * co.y);
                 v[0] -= dm0;  // d(mean) = -d(delta)
                 v[1] -= dm1;
-                v[9] += sqrtf(dm0 * dm0 + dm1 * dm1);
+                v[9] += sqrt_approx(dm0 * dm0 + dm1 * dm1);
                 v[2] += -0.5f * dL_dweight * gx * dx;
                 v[3] += -dL_dweight * gx * dy;
                 v[4] += -0.5f * dL_dweight * gy * dy;
@@ -419,7 +429,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
             v[3] = d3.x + d3.y;
             v[4] = d4.x + d4.y;
             v[5] = q.x + q.y;
-            v[9] = sqrtf(sq.x) + sqrtf(sq.y);
+            v[9] = sqrt_approx(sq.x) + sqrt_approx(sq.y);
           }
         }
       }
