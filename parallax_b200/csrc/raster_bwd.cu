@@ -243,63 +243,93 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
   }
 }
 
-// The two-pixel form of k_backward: the gradient arithmetic of the two
-// vertically adjacent pixels of a thread runs as the halves of paired FP32
-// instructions (fma/add/mul .f32x2). The branch decisions are the forward's,
-// from the same scalar operations (splat_power2, alpha = opacity * exp). A
-// pixel that does not take an entry runs the paired arithmetic with alpha = 0
-// and a zero loss gradient, so its transmittance (multiplied by 1), its suffix
-// colour (an FMA with a zero weight) and its sums are unchanged.
-__global__ void __launch_bounds__(TileGeom<2>::kThreads)
-    k_backward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
-                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
-                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,
-                  int n_views, const float* __restrict__ T_final,
-                  const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
-                  ScreenGrad* __restrict__ screen, const uint8_t* __restrict__ block_bits) {
-  constexpr int kThreads = TileGeom<2>::kThreads;
-  __shared__ uint32_t s_slot[kBatch];
-  __shared__ float2 s_xy[kBatch];
-  __shared__ float4 s_co[kBatch];
-  __shared__ float4 s_col[kBatch];  // r, g, b, power floor
-  __shared__ uint32_t s_mask[kBatch];
-  __shared__ float s_acc[kBatch][12];
-  __shared__ uint8_t s_list[TileGeom<2>::kWarps][kBatch];  // a warp's entries of the batch
+// Warp w's bit in a tile-list entry's mask for the adjoint with PX pixels per
+// thread, from the forward's block bits (bit b: some pixel of 8x8 block b of
+// the two-pixel layout took the entry). With four pixels per thread warp w
+// covers the two-pixel blocks w and w + 2.
+template <int PX>
+__device__ __forceinline__ uint32_t mask_from_block_bits(uint32_t bits) {
+  if constexpr (PX == 2) return bits;
+  else return (bits | (bits >> 2)) & 3u;
+}
+
+// The paired-FP32 forms of k_backward, with NP pairs of vertically adjacent
+// pixels per thread (NP = 1: two pixels, 8x8 blocks per warp; NP = 2: four
+// pixels, 8x16 blocks). The gradient arithmetic of a pair runs as the halves
+// of paired FP32 instructions (fma/add/mul .f32x2). The branch decisions are
+// the forward's, from the same scalar operations (splat_power2, alpha =
+// opacity * exp). A pixel that does not take an entry runs the paired
+// arithmetic with alpha = 0 and a zero loss gradient, so its transmittance
+// (multiplied by 1), its suffix colour (an FMA with a zero weight) and its
+// sums are unchanged. A thread adds its pairs' contributions before the warp
+// reduction, so one reduction serves 2 NP pixels per lane.
+template <int NP>
+__global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
+    k_backward_pairs(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
+                     const float2* __restrict__ xy, const float4* __restrict__ conic_op,
+                     const float4* __restrict__ color, const ViewDesc* __restrict__ views,
+                     int n_views, const float* __restrict__ T_final,
+                     const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
+                     ScreenGrad* __restrict__ screen, const uint8_t* __restrict__ block_bits) {
+  constexpr int PX = 2 * NP;
+  constexpr int kThreads = TileGeom<PX>::kThreads;
+  constexpr int kWarps = TileGeom<PX>::kWarps;
+  // fewer threads share a batch with more pixels each: a smaller batch keeps
+  // the shared memory per warp, and so the resident warps, about the same
+  constexpr int kB = NP == 1 ? kBatch : kBatch / 2;
+  __shared__ uint32_t s_slot[kB];
+  __shared__ float2 s_xy[kB];
+  __shared__ float4 s_co[kB];
+  __shared__ float4 s_col[kB];  // r, g, b, power floor
+  __shared__ uint32_t s_mask[kB];
+  __shared__ float s_acc[kB][12];
+  __shared__ uint8_t s_list[kWarps][kB];  // a warp's entries of the batch
   __shared__ int s_hi;
-  static_assert(kBatch <= 256, "batch indices are bytes");
-  const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
+  static_assert(kB <= 256, "batch indices are bytes");
+  const TileInfo<PX> info = tile_info<PX>(views, n_views, ranges);
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha;
   const float fx = (float)info.px + 0.5f;
-  const float2 fy = make_float2((float)info.py0 + 0.5f, (float)(info.py0 + 1) + 0.5f);
-  float2 dLp0 = make_float2(0.f, 0.f), dLp1 = dLp0, dLp2 = dLp0;
-  float2 T = make_float2(1.f, 1.f);
-  int last0 = info.range.x, last1 = info.range.x;
+  const float2 zero2 = make_float2(0.f, 0.f);
+  float2 fy[NP], dLp0[NP], dLp1[NP], dLp2[NP], T[NP], bg_term[NP];
+  int last0[NP], last1[NP];
+  int hi_mine = info.range.x;
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    const int py = info.py0 + p;
-    if (info.px < vd.cam.width && py < vd.cam.height) {
-      const int64_t pixel = vd.pixel_offset + (int64_t)py * vd.cam.width + info.px;
-      const float d0 = dL_drgb[pixel * 3 + 0], d1 = dL_drgb[pixel * 3 + 1];
-      const float d2 = dL_drgb[pixel * 3 + 2], tf = T_final[pixel];
-      const int l = last_in[pixel];
-      if (p == 0) {
-        dLp0.x = d0; dLp1.x = d1; dLp2.x = d2; T.x = tf; last0 = l;
-      } else {
-        dLp0.y = d0; dLp1.y = d1; dLp2.y = d2; T.y = tf; last1 = l;
+  for (int q = 0; q < NP; ++q) {
+    const int py = info.py0 + 2 * q;
+    fy[q] = make_float2((float)py + 0.5f, (float)(py + 1) + 0.5f);
+    dLp0[q] = dLp1[q] = dLp2[q] = zero2;
+    T[q] = make_float2(1.f, 1.f);
+    last0[q] = last1[q] = info.range.x;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      if (info.px < vd.cam.width && py + p < vd.cam.height) {
+        const int64_t pixel = vd.pixel_offset + (int64_t)(py + p) * vd.cam.width + info.px;
+        const float d0 = dL_drgb[pixel * 3 + 0], d1 = dL_drgb[pixel * 3 + 1];
+        const float d2 = dL_drgb[pixel * 3 + 2], tf = T_final[pixel];
+        const int l = last_in[pixel];
+        if (p == 0) {
+          dLp0[q].x = d0; dLp1[q].x = d1; dLp2[q].x = d2; T[q].x = tf; last0[q] = l;
+        } else {
+          dLp0[q].y = d0; dLp1[q].y = d1; dLp2[q].y = d2; T[q].y = tf; last1[q] = l;
+        }
       }
     }
+    // final T times the background's share of the loss gradient
+    bg_term[q] = __fmul2_rn(
+        T[q], __ffma2_rn(make_float2(vd.background[2], vd.background[2]), dLp2[q],
+                         __ffma2_rn(make_float2(vd.background[1], vd.background[1]), dLp1[q],
+                                    __fmul2_rn(make_float2(vd.background[0],
+                                                           vd.background[0]),
+                                               dLp0[q]))));
+    hi_mine = max(hi_mine, max(last0[q], last1[q]));
   }
-  // final T times the background's share of the loss gradient
-  const float2 bg_term = __fmul2_rn(
-      T, __ffma2_rn(make_float2(vd.background[2], vd.background[2]), dLp2,
-                    __ffma2_rn(make_float2(vd.background[1], vd.background[1]), dLp1,
-                               __fmul2_rn(make_float2(vd.background[0], vd.background[0]),
-                                          dLp0))));
-  float2 suffix0 = make_float2(0.f, 0.f), suffix1 = suffix0, suffix2 = suffix0;
-  float2 last_alpha = suffix0, lc0 = suffix0, lc1 = suffix0, lc2 = suffix0;
+  float2 suffix0[NP], suffix1[NP], suffix2[NP], last_alpha[NP], lc0[NP], lc1[NP], lc2[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q)
+    suffix0[q] = suffix1[q] = suffix2[q] = last_alpha[q] = lc0[q] = lc1[q] = lc2[q] = zero2;
   const int lane = lane_id(), warp = warp_id();
-  const int warp_hi = __reduce_max_sync(kFull, max(last0, last1));
+  const int warp_hi = __reduce_max_sync(kFull, hi_mine);
   if (threadIdx.x == 0) s_hi = info.range.x;
   __syncthreads();
   if (lane == 0 && warp_hi > info.range.x) atomicMax(&s_hi, warp_hi);
@@ -307,8 +337,8 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
   const int hi = s_hi;
   const float2 one = make_float2(1.f, 1.f);
 
-  for (int batch_end = hi; batch_end > info.range.x; batch_end -= kBatch) {
-    const int batch_start = max(info.range.x, batch_end - kBatch);
+  for (int batch_end = hi; batch_end > info.range.x; batch_end -= kB) {
+    const int batch_start = max(info.range.x, batch_end - kB);
     const int n = batch_end - batch_start;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += kThreads) {
@@ -324,14 +354,15 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
       // which warps took the entry in the forward pass (exact), else which
       // ones its footprint can reach
       s_mask[i] = block_bits != nullptr
-                      ? (uint32_t)block_bits[batch_start + i]
-                      : warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
+                      ? mask_from_block_bits<PX>(block_bits[batch_start + i])
+                      : warp_mask<PX>(mean, co, c.w, info.tile_px, info.tile_py);
 #pragma unroll
       for (int k = 0; k < 12; ++k) s_acc[i][k] = 0.f;
     }
     __syncthreads();
     const int j_top = min(n, warp_hi - batch_start) - 1;  // warp-uniform
-    // the entries some pixel of this warp takes (or can reach), ascending
+    // the entries some pixel of this warp takes (or can reach), ascending;
+    // built by the whole warp, which is converged here
     int n_mine = 0;
     for (int j0 = 0; j0 <= j_top; j0 += 32) {
       const int jj = j0 + lane;
@@ -341,22 +372,29 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
       n_mine += __popc(b);
     }
     __syncwarp();
-    for (int q = n_mine - 1; q >= 0; --q) {  // back to front
-      const int j = s_list[warp][q];
+    for (int qi = n_mine - 1; qi >= 0; --qi) {  // back to front
+      const int j = s_list[warp][qi];
       const int e = batch_start + j;
       const float2 m = s_xy[j];
       const float4 co = s_co[j];
       const float4 c = s_col[j];
       const float dx = fx - m.x;
-      const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
-      const float2 power = splat_power2(co, dx, dy);
-      const bool in0 = e < last0 && !(power.x > 0.f) && !(power.x < c.w);
-      const bool in1 = e < last1 && !(power.y > 0.f) && !(power.y < c.w);
       bool contrib = false, touched = false;
       float v[10];
 #pragma unroll
       for (int k = 0; k < 10; ++k) v[k] = 0.f;
-      if (in0 || in1) {
+      // pair q's sums into v: assigned by the first pair, added by the next
+      auto put = [&](int q, int k, float x) {
+        if (q == 0) v[k] = x;
+        else v[k] += x;
+      };
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        const float2 dy = make_float2(fy[q].x - m.y, fy[q].y - m.y);
+        const float2 power = splat_power2(co, dx, dy);
+        const bool in0 = e < last0[q] && !(power.x > 0.f) && !(power.x < c.w);
+        const bool in1 = e < last1[q] && !(power.y > 0.f) && !(power.y < c.w);
+        if (!(in0 || in1)) continue;
         const float g0 = in0 ? expf(power.x) : 0.f;
         const float g1 = in1 ? expf(power.y) : 0.f;
         const float r0 = __fmul_rn(co.w, g0), r1 = __fmul_rn(co.w, g1);
@@ -364,74 +402,73 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
         const float a1 = r1 < kMaxAlpha ? r1 : kMaxAlpha;
         const bool c0 = in0 && !(a0 < min_alpha);
         const bool c1 = in1 && !(a1 < min_alpha);
-        if (c0 || c1) {
-          contrib = true;
-          const float2 alpha = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
-          const float2 inv = make_float2(c0 ? __fdividef(1.f, 1.f - alpha.x) : 1.f,
-                                         c1 ? __fdividef(1.f, 1.f - alpha.y) : 1.f);
-          T = __fmul2_rn(T, inv);
-          const float2 weight = __fmul2_rn(alpha, T);
-          const float2 w6 = __fmul2_rn(weight, dLp0);
-          const float2 w7 = __fmul2_rn(weight, dLp1);
-          const float2 w8 = __fmul2_rn(weight, dLp2);
-          v[6] = w6.x + w6.y;
-          v[7] = w7.x + w7.y;
-          v[8] = w8.x + w8.y;
-          // suffix = la * lc + (1 - la) * suffix, only where this entry counts
-          const float2 la = make_float2(c0 ? last_alpha.x : 0.f, c1 ? last_alpha.y : 0.f);
-          const float2 keep = __fadd2_rn(one, make_float2(-la.x, -la.y));
-          suffix0 = __ffma2_rn(la, lc0, __fmul2_rn(keep, suffix0));
-          suffix1 = __ffma2_rn(la, lc1, __fmul2_rn(keep, suffix1));
-          suffix2 = __ffma2_rn(la, lc2, __fmul2_rn(keep, suffix2));
-          if (c0) {
-            lc0.x = c.x; lc1.x = c.y; lc2.x = c.z; last_alpha.x = alpha.x;
-          }
-          if (c1) {
-            lc0.y = c.x; lc1.y = c.y; lc2.y = c.z; last_alpha.y = alpha.y;
-          }
-          float2 dL_dalpha = __fmul2_rn(
-              __ffma2_rn(__fadd2_rn(make_float2(c.z, c.z), make_float2(-suffix2.x, -suffix2.y)),
-                         dLp2,
-                         __ffma2_rn(__fadd2_rn(make_float2(c.y, c.y),
-                                               make_float2(-suffix1.x, -suffix1.y)),
-                                    dLp1,
-                                    __fmul2_rn(__fadd2_rn(make_float2(c.x, c.x),
-                                                          make_float2(-suffix0.x, -suffix0.y)),
-                                               dLp0))),
-              T);
-          dL_dalpha = __ffma2_rn(make_float2(-inv.x, -inv.y), bg_term, dL_dalpha);
-          // the 0.99 cap flattens the gradient
-          const bool t0 = c0 && r0 < kMaxAlpha, t1 = c1 && r1 < kMaxAlpha;
-          if (t0 || t1) {
-            touched = true;
-            const float2 z = make_float2(t0 ? dL_dalpha.x : 0.f, t1 ? dL_dalpha.y : 0.f);
-            const float2 gw = make_float2(g0, g1);
-            const float2 q = __fmul2_rn(gw, z);          // dL/dopacity per pixel
-            const float2 dLw = __fmul2_rn(make_float2(co.w, co.w), z);
-            const float2 gx = __fmul2_rn(gw, make_float2(dx, dx));
-            const float2 gy = __fmul2_rn(gw, dy);
-            // d(mean) = -d(delta): v0 = -dm0, v1 = -dm1
-            const float2 dm0 = __fmul2_rn(
-                dLw, __ffma2_rn(gy, make_float2(-co.y, -co.y),
-                                __fmul2_rn(gx, make_float2(-co.x, -co.x))));
-            const float2 dm1 = __fmul2_rn(
-                dLw, __ffma2_rn(gx, make_float2(-co.y, -co.y),
-                                __fmul2_rn(gy, make_float2(-co.z, -co.z))));
-            const float2 sq = __ffma2_rn(dm1, dm1, __fmul2_rn(dm0, dm0));
-            const float2 wx = __fmul2_rn(dLw, gx);
-            const float2 wy = __fmul2_rn(dLw, gy);
-            const float2 d2 = __fmul2_rn(wx, make_float2(-0.5f * dx, -0.5f * dx));
-            const float2 d3 = __fmul2_rn(wx, make_float2(-dy.x, -dy.y));
-            const float2 d4 = __fmul2_rn(wy, __fmul2_rn(make_float2(-0.5f, -0.5f), dy));
-            v[0] = -(dm0.x + dm0.y);
-            v[1] = -(dm1.x + dm1.y);
-            v[2] = d2.x + d2.y;
-            v[3] = d3.x + d3.y;
-            v[4] = d4.x + d4.y;
-            v[5] = q.x + q.y;
-            v[9] = sqrt_approx(sq.x) + sqrt_approx(sq.y);
-          }
+        if (!(c0 || c1)) continue;
+        contrib = true;
+        const float2 alpha = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
+        const float2 inv = make_float2(c0 ? __fdividef(1.f, 1.f - alpha.x) : 1.f,
+                                       c1 ? __fdividef(1.f, 1.f - alpha.y) : 1.f);
+        T[q] = __fmul2_rn(T[q], inv);
+        const float2 weight = __fmul2_rn(alpha, T[q]);
+        const float2 w6 = __fmul2_rn(weight, dLp0[q]);
+        const float2 w7 = __fmul2_rn(weight, dLp1[q]);
+        const float2 w8 = __fmul2_rn(weight, dLp2[q]);
+        put(q, 6, w6.x + w6.y);
+        put(q, 7, w7.x + w7.y);
+        put(q, 8, w8.x + w8.y);
+        // suffix = la * lc + (1 - la) * suffix, only where this entry counts
+        const float2 la = make_float2(c0 ? last_alpha[q].x : 0.f, c1 ? last_alpha[q].y : 0.f);
+        const float2 keep = __fadd2_rn(one, make_float2(-la.x, -la.y));
+        suffix0[q] = __ffma2_rn(la, lc0[q], __fmul2_rn(keep, suffix0[q]));
+        suffix1[q] = __ffma2_rn(la, lc1[q], __fmul2_rn(keep, suffix1[q]));
+        suffix2[q] = __ffma2_rn(la, lc2[q], __fmul2_rn(keep, suffix2[q]));
+        if (c0) {
+          lc0[q].x = c.x; lc1[q].x = c.y; lc2[q].x = c.z; last_alpha[q].x = alpha.x;
         }
+        if (c1) {
+          lc0[q].y = c.x; lc1[q].y = c.y; lc2[q].y = c.z; last_alpha[q].y = alpha.y;
+        }
+        float2 dL_dalpha = __fmul2_rn(
+            __ffma2_rn(
+                __fadd2_rn(make_float2(c.z, c.z), make_float2(-suffix2[q].x, -suffix2[q].y)),
+                dLp2[q],
+                __ffma2_rn(
+                    __fadd2_rn(make_float2(c.y, c.y), make_float2(-suffix1[q].x, -suffix1[q].y)),
+                    dLp1[q],
+                    __fmul2_rn(__fadd2_rn(make_float2(c.x, c.x),
+                                          make_float2(-suffix0[q].x, -suffix0[q].y)),
+                               dLp0[q]))),
+            T[q]);
+        dL_dalpha = __ffma2_rn(make_float2(-inv.x, -inv.y), bg_term[q], dL_dalpha);
+        // the 0.99 cap flattens the gradient
+        const bool t0 = c0 && r0 < kMaxAlpha, t1 = c1 && r1 < kMaxAlpha;
+        if (!(t0 || t1)) continue;
+        touched = true;
+        const float2 z = make_float2(t0 ? dL_dalpha.x : 0.f, t1 ? dL_dalpha.y : 0.f);
+        const float2 gw = make_float2(g0, g1);
+        const float2 qo = __fmul2_rn(gw, z);  // dL/dopacity per pixel
+        const float2 dLw = __fmul2_rn(make_float2(co.w, co.w), z);
+        const float2 gx = __fmul2_rn(gw, make_float2(dx, dx));
+        const float2 gy = __fmul2_rn(gw, dy);
+        // d(mean) = -d(delta): v0 = -dm0, v1 = -dm1
+        const float2 dm0 = __fmul2_rn(
+            dLw, __ffma2_rn(gy, make_float2(-co.y, -co.y),
+                            __fmul2_rn(gx, make_float2(-co.x, -co.x))));
+        const float2 dm1 = __fmul2_rn(
+            dLw, __ffma2_rn(gx, make_float2(-co.y, -co.y),
+                            __fmul2_rn(gy, make_float2(-co.z, -co.z))));
+        const float2 sq = __ffma2_rn(dm1, dm1, __fmul2_rn(dm0, dm0));
+        const float2 wx = __fmul2_rn(dLw, gx);
+        const float2 wy = __fmul2_rn(dLw, gy);
+        const float2 d2 = __fmul2_rn(wx, make_float2(-0.5f * dx, -0.5f * dx));
+        const float2 d3 = __fmul2_rn(wx, make_float2(-dy.x, -dy.y));
+        const float2 d4 = __fmul2_rn(wy, __fmul2_rn(make_float2(-0.5f, -0.5f), dy));
+        put(q, 0, -(dm0.x + dm0.y));
+        put(q, 1, -(dm1.x + dm1.y));
+        put(q, 2, d2.x + d2.y);
+        put(q, 3, d3.x + d3.y);
+        put(q, 4, d4.x + d4.y);
+        put(q, 5, qo.x + qo.y);
+        put(q, 9, sqrt_approx(sq.x) + sqrt_approx(sq.y));
       }
       const unsigned ballot = __ballot_sync(kFull, contrib);
       if (ballot != 0u) {
@@ -494,11 +531,12 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
                      T_final, last, dL_drgb, screen, stream);
       break;
     case 4:
-      backward_px<4>(ranges, pair_slots, xy, conic_op, color, views, n_views, total_tiles,
-                     T_final, last, dL_drgb, screen, stream);
+      k_backward_pairs<2><<<total_tiles, TileGeom<4>::kThreads, 0, stream>>>(
+          ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
+          screen, block_bits);
       break;
     default:
-      k_backward_x2<<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
+      k_backward_pairs<1><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
           ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
           screen, block_bits);
   }
