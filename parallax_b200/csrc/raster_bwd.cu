@@ -27,16 +27,6 @@ constexpr int kDirectLanes = 2;
 
 // Sums v[0..9] over the warp. Returns, in ten of the even lanes, one complete
 // sum; *idx is the index of that value, or -1 in the other lanes.
-// |d(mean)| for the densification statistic (the sum of per-pixel gradient
-// norms compared against a threshold): the hardware square root
-// approximation (relative error about 2^-22) instead of the correctly
-// rounded one, which costs several instructions more per pixel.
-__device__ __forceinline__ float sqrt_approx(float x) {
-  float r;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-
 __device__ __forceinline__ float warp_reduce10(const float (&v)[10], int lane, int* idx) {
   const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
   float w[6];
@@ -468,6 +458,8 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         put(q, 3, d3.x + d3.y);
         put(q, 4, d4.x + d4.y);
         put(q, 5, qo.x + qo.y);
+        // |d(mean)| for the densification statistic (a sum of per-pixel norms
+        // compared against a threshold): the square-root approximation
         put(q, 9, sqrt_approx(sq.x) + sqrt_approx(sq.y));
       }
       const unsigned ballot = __ballot_sync(kFull, contrib);

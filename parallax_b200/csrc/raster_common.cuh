@@ -50,6 +50,13 @@ __device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ v
   return info;
 }
 
+// The hardware square-root approximation (relative error about 2^-22).
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Bit w is set when some pixel of warp w's block may see this splat with
 // power >= `floor` (and so possibly alpha >= min_alpha). The region
 // {d : d^T A d <= -2 floor} of the conic A lies in the box
@@ -64,9 +71,11 @@ __device__ __forceinline__ uint32_t warp_mask(float2 mean, const float4& co, flo
   if (!(floor > -1e30f)) return kAll;
   const float det = co.x * co.z - co.y * co.y;
   if (!(det > 0.f)) return kAll;
+  // hardware approximations (relative error ~1e-7): the 10% widening covers them
   const float k = -2.f * floor;
-  const float ex = sqrtf(k * co.z / det) * 1.1f + 0.5f;
-  const float ey = sqrtf(k * co.x / det) * 1.1f + 0.5f;
+  const float inv_det = __fdividef(1.f, det);
+  const float ex = sqrt_approx(k * co.z * inv_det) * 1.1f + 0.5f;
+  const float ey = sqrt_approx(k * co.x * inv_det) * 1.1f + 0.5f;
   if (!(ex < 1e4f && ey < 1e4f)) return kAll;
   uint32_t m = 0u;
 #pragma unroll
@@ -105,12 +114,13 @@ __device__ __forceinline__ float2 splat_power2(const float4& co, float dx, float
 }
 
 // A power below which opacity * exp(power) is certainly under min_alpha, so
-// exp need not be evaluated: ln(min_alpha / opacity) less a 1e-5 margin that
-// covers the rounding of logf, expf and the product (all far below 1e-6 in
-// log space for the |ln| <= 5.6 that opacity >= min_alpha allows). -inf when
+// exp need not be evaluated: ln(min_alpha / opacity) less a 1e-5 margin. The
+// quotient and the log are the hardware approximations (at most 3 ulp, under
+// 2e-6 in log space for the |ln| <= 5.6 that opacity >= min_alpha allows);
+// the margin covers them and the rounding of expf and the product. -inf when
 // min_alpha is 0.
 __device__ __forceinline__ float power_floor(float opacity, float min_alpha) {
-  return logf(min_alpha / opacity) - 1e-5f;
+  return __logf(__fdividef(min_alpha, opacity)) - 1e-5f;
 }
 
 }  // namespace pxs
