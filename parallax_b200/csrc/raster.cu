@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads)
       s_xy[i] = mean;
       s_co[i] = co;
       s_col[i] = c;
-      s_mask[i] = warp_mask<2>(mean, co, c.w, info.tile_px, info.tile_py);
+      s_mask[i] = warp_mask<2, true>(mean, co, c.w, info.tile_px, info.tile_py);
     }
     __syncthreads();
     // entry j for this warp's pixels; returns whether both are done

@@ -57,14 +57,35 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return r;
 }
 
+// The least q(dx, dy) = a dx^2 + 2 b dx dy + c dy^2 of a conic (a, b, c) =
+// (co.x, co.y, co.z), positive definite, over the rectangle [dx0, dx1] x
+// [dy0, dy1]: 0 when it holds the origin, else on its boundary, where each
+// edge's least value is at the edge's stationary point clamped to the edge.
+__device__ __forceinline__ float rect_min_q(const float4& co, float dx0, float dx1, float dy0,
+                                            float dy1) {
+  if (dx0 <= 0.f && dx1 >= 0.f && dy0 <= 0.f && dy1 >= 0.f) return 0.f;
+  const float a = co.x, b = co.y, c = co.z;
+  const float ia = __fdividef(1.f, a), ic = __fdividef(1.f, c);
+  auto q = [&](float x, float y) { return a * x * x + 2.f * b * x * y + c * y * y; };
+  auto clampf = [](float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); };
+  float best = q(dx0, clampf(-b * dx0 * ic, dy0, dy1));
+  best = fminf(best, q(dx1, clampf(-b * dx1 * ic, dy0, dy1)));
+  best = fminf(best, q(clampf(-b * dy0 * ia, dx0, dx1), dy0));
+  best = fminf(best, q(clampf(-b * dy1 * ia, dx0, dx1), dy1));
+  return best;
+}
+
 // Bit w is set when some pixel of warp w's block may see this splat with
-// power >= `floor` (and so possibly alpha >= min_alpha). The region
+// power >= `floor` (and so possibly alpha >= min_alpha), i.e. q = -2 power <=
+// k = -2 floor somewhere in the block. The region
 // {d : d^T A d <= -2 floor} of the conic A lies in the box
 // |dx| <= sqrt(-2 floor (A^-1)_xx), |dy| <= sqrt(-2 floor (A^-1)_yy); the box is
 // widened by 10% and half a pixel, which covers the rounding of the computed
 // power for any splat narrower than ~1000 px of standard deviation (wider ones
-// get every bit). No floor (min_alpha = 0) sets every bit.
-template <int PX>
+// get every bit). No floor (min_alpha = 0) sets every bit. With kRefine the
+// box's blocks are tested against the ellipse itself (below); it costs
+// registers, so only the compositing pass, which walks by these masks, uses it.
+template <int PX, bool kRefine = false>
 __device__ __forceinline__ uint32_t warp_mask(float2 mean, const float4& co, float floor,
                                               int tile_px, int tile_py) {
   constexpr uint32_t kAll = (1u << TileGeom<PX>::kWarps) - 1u;
@@ -77,6 +98,14 @@ __device__ __forceinline__ uint32_t warp_mask(float2 mean, const float4& co, flo
   const float ex = sqrt_approx(k * co.z * inv_det) * 1.1f + 0.5f;
   const float ey = sqrt_approx(k * co.x * inv_det) * 1.1f + 0.5f;
   if (!(ex < 1e4f && ey < 1e4f)) return kAll;
+  // a block whose box test passes is then dropped when the least q over its
+  // rectangle of pixel centres exceeds k: the footprint ellipse misses it
+  // although the box does not. Only for conics with a c < 10 det (|rho| <=
+  // 0.95): the absolute terms of q then sum to at most 38 q, so the float
+  // rounding of q, here and in the kernels' per-pixel power, stays ten times
+  // under the margin below. More elongated splats keep the box test alone.
+  const bool refine = kRefine && co.x * co.z < 10.f * det;
+  const float q_cut = k * 1.0001f + 1e-4f;
   uint32_t m = 0u;
 #pragma unroll
   for (int w = 0; w < TileGeom<PX>::kWarps; ++w) {
@@ -84,7 +113,9 @@ __device__ __forceinline__ uint32_t warp_mask(float2 mean, const float4& co, flo
     const float y_lo = (float)(tile_py + (w >> 1) * TileGeom<PX>::kBlockH) + 0.5f;
     const float y_hi = y_lo + (float)(TileGeom<PX>::kBlockH - 1);
     if (x_lo <= mean.x + ex && x_hi >= mean.x - ex && y_lo <= mean.y + ey &&
-        y_hi >= mean.y - ey)
+        y_hi >= mean.y - ey &&
+        !(refine &&
+          rect_min_q(co, x_lo - mean.x, x_hi - mean.x, y_lo - mean.y, y_hi - mean.y) > q_cut))
       m |= 1u << w;
   }
   return m;
