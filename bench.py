@@ -604,15 +604,6 @@ def run_multi_scene(args):
     trainer = px.SplatTrainer.from_scenes(starts, scene_views, cfg, device=local)
     n_views = sum(len(v) for v in scene_views)
     ids = list(range(n_views))
-    def ingest(ids):
-        id_arr = (ct.c_int32 * len(ids))(*ids)
-        ptrs = (ct.c_void_p * len(ids))(*[frames[i].data_ptr() for i in ids])
-        ws = (ct.c_int32 * len(ids))(*[views[i].width for i in ids])
-        hs = (ct.c_int32 * len(ids))(*[views[i].height for i in ids])
-        trainer._check(lib.pxs_trainer_ingest_images(trainer.handle, len(ids), id_arr, ptrs,
-                                                     ws, hs))
-
-    ingest(list(range(len(views))))
     sp = ct.c_void_p()
     trainer._check(lib.pxs_trainer_stream(trainer.handle, ct.byref(sp)))
     stream = torch.cuda.ExternalStream(sp.value)
