@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     if (want_ssim) {
       // horizontal blur of the five products over every input row, onto the
-      // statistics columns; a thread slides the 11 taps over 6 outputs
-      constexpr int HS = 6;
+      // statistics columns; a thread slides the 11 taps over 7 outputs
+      constexpr int HS = 7;
       for (int item = tid; item < IH * (SW / HS); item += kThreads) {
         const int r = item / (SW / HS), col0 = (item % (SW / HS)) * HS;
         float xs[HS + 10], ys[HS + 10], xx[HS + 10], yy[HS + 10], xy[HS + 10];
@@ -136,8 +136,8 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
       __syncthreads();
       // vertical blur -> statistics, then the SSIM map and its partials in
-      // place; a thread takes one column and 6 consecutive rows
-      constexpr int VS = 6;
+      // place; a thread takes one column and 7 consecutive rows
+      constexpr int VS = 7;
       constexpr int VSEG = (SH + VS - 1) / VS;
       for (int item = tid; item < SW * VSEG; item += kThreads) {
         const int col = item % SW, r0 = (item / SW) * VS;
