@@ -191,8 +191,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
       }
       __syncthreads();
-      // horizontal blur of the partials onto the tile's columns, 8 per thread
-      constexpr int HS2 = 8;
+      // horizontal blur of the partials onto the tile's columns, 16 per thread
+      constexpr int HS2 = 16;
       for (int item = tid; item < 3 * SH * (TW / HS2); item += kThreads) {
         const int p = item / (SH * (TW / HS2));
         const int rem = item % (SH * (TW / HS2));
