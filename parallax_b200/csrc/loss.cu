@@ -28,7 +28,7 @@ namespace {
 constexpr int TW = 32, TH = 32;
 constexpr int IW = TW + 20, IH = TH + 20;  // input region
 constexpr int SW = TW + 10, SH = TH + 10;  // statistics region
-constexpr int kThreads = 256;
+constexpr int kThreads = 320;  // every blur pass below is one round of items
 
 struct LossSmem {
   float in_r[IH][IW];      // rendered, the current channel
