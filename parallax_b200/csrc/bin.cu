@@ -8,7 +8,7 @@
 //   1. each visible splat has one record per tile row it covers (about one
 //      seventh as many as pairs), wanted grouped by row and near to far
 //      within a row: each view's depth-sorted slots are cut into chunks of
-//      512; a CTA per chunk counts, per tile row, the splats covering it; an
+//      1024; a CTA per chunk counts, per tile row, the splats covering it; an
 //      exclusive scan of the counts in (row, chunk) order gives each chunk
 //      its base in each row, and the chunk writes its records there (the
 //      ranking of step 3 with rows for columns) -- a stable counting sort by
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 // chunk its base in every row; the chunk then writes its records there with
 // the same bitmap ranking and staging as the tile lists (rows for columns).
 // This is the stable counting sort of the records by row, with no sort pass.
-constexpr int kSlotChunk = 512;
+constexpr int kSlotChunk = 1024;
 constexpr int kSlotPerLane = kSlotChunk / (kWarps * 32);  // slots per lane per chunk
 
 // Lane slots of a chunk starting at `begin` of the depth-sorted slots, and
