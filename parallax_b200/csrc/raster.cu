@@ -156,13 +156,17 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 9)
                  int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts,
                  uint8_t* __restrict__ block_bits) {
   constexpr int kThreads = TileGeom<2>::kThreads;
-  __shared__ float2 s_xy[kBatch];
-  __shared__ float4 s_co[kBatch];
-  __shared__ float4 s_col[kBatch];  // r, g, b, power floor
-  __shared__ uint32_t s_mask[kBatch];
-  __shared__ uint8_t s_took[TileGeom<2>::kWarps][kBatch];  // warp w = 8x8 block w
-  __shared__ uint8_t s_list[TileGeom<2>::kWarps][kBatch];  // a warp's entries of the batch
-  static_assert(kBatch <= 256, "batch indices are bytes");
+  // half the adjoint's batch: a tile stops at saturation, so a smaller batch
+  // stages fewer entries past it (the adjoint walks to each pixel's last
+  // contributor and keeps the larger batch)
+  constexpr int kFwdBatch = kBatch / 2;
+  __shared__ float2 s_xy[kFwdBatch];
+  __shared__ float4 s_co[kFwdBatch];
+  __shared__ float4 s_col[kFwdBatch];  // r, g, b, power floor
+  __shared__ uint32_t s_mask[kFwdBatch];
+  __shared__ uint8_t s_took[TileGeom<2>::kWarps][kFwdBatch];  // warp w = 8x8 block w
+  __shared__ uint8_t s_list[TileGeom<2>::kWarps][kFwdBatch];  // a warp's entries of the batch
+  static_assert(kFwdBatch <= 256, "batch indices are bytes");
   const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
   const int warp = threadIdx.x >> 5;
   const ViewDesc& vd = views[info.view];
@@ -183,7 +187,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 9)
       block_bits[prev_base + i] = (uint8_t)(s_took[0][i] | (s_took[1][i] << 1) |
                                             (s_took[2][i] << 2) | (s_took[3][i] << 3));
   };
-  for (int base = info.range.x; base < info.range.y; base += kBatch) {
+  for (int base = info.range.x; base < info.range.y; base += kFwdBatch) {
     const bool all_done = __syncthreads_and(done0 && done1);
     if (kBits) {
       write_bits();
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 9)
     }
     if (all_done) break;
     if (kBits) __syncthreads();  // the bits are read before they are cleared
-    const int n = min(kBatch, info.range.y - base);
+    const int n = min(kFwdBatch, info.range.y - base);
     for (int i = threadIdx.x; i < n; i += kThreads) {
       if (kBits) {
 #pragma unroll
