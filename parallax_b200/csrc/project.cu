@@ -24,7 +24,7 @@ constexpr int kProjectThreads = 256;
 // coefficients per channel are read together into this thread's column of
 // shared memory and serve every view.
 template <int S>
-__global__ void __launch_bounds__(kProjectThreads)
+__global__ void __launch_bounds__(kProjectThreads, 3)
     k_project(const float* __restrict__ params, int N, int64_t slot_stride,
               const ViewDesc* __restrict__ views, int n_views, ProjectedSoA out) {
   constexpr int kRest = 3 * S > 0 ? 3 * S : 1;
