@@ -23,7 +23,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 // At most this many contributing lanes: per-lane shared-memory atomics
 // instead of the warp-wide transpose reduction.
-constexpr int kDirectLanes = 2;
+constexpr int kDirectLanes = 1;
 
 // Sums v[0..9] over the warp. Returns, in ten of the even lanes, one complete
 // sum; *idx is the index of that value, or -1 in the other lanes.
