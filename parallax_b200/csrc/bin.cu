@@ -47,7 +47,7 @@ __device__ __forceinline__ int view_of_row(const ViewDesc* __restrict__ views, i
 // whatever the rows' lengths. chunks[c] = (row, begin, end); n_chunks[0] is
 // the count. One CTA builds the table with a block-wide scan over the rows.
 constexpr int kChunk = 1024;
-constexpr int kStage = 8192;  // pairs a chunk can stage in shared memory
+constexpr int kStage = 10240;  // pairs a chunk can stage in shared memory
 constexpr int kPerLane = kChunk / (kWarps * 32);  // records per lane per chunk
 
 __global__ void __launch_bounds__(1024)
