@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
 // multiply and add by at most one rounding per entry. A pixel that does not
 // take an entry adds T * 0 * colour = 0.
 template <bool kCount, bool kBits>
-__global__ void __launch_bounds__(TileGeom<2>::kThreads, 9)
+__global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
     k_forward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,
