@@ -370,3 +370,104 @@ int32_t pxo_densify_and_prune(float* params, int32_t n, int32_t rest_per_channel
   free(keep);
   return (int32_t)count;
 }
+
+/* ---------------------------------------------- per-pixel decision margins
+ *
+ * The compositing loop of rasterizeSplats (SplatRaster.cpp:285-303) makes
+ * four threshold decisions per evaluated entry: power > 0 (skip), the cap of
+ * alpha at 0.99, alpha < min_alpha (skip) and, after the multiply,
+ * T < transmittance_cutoff (stop). Two implementations whose inputs differ in
+ * the last bit (glibc's expf is not correctly rounded everywhere; sums round
+ * in a different order) can take a decision the other way and change a pixel
+ * by far more than their rounding. For every pixel this walks the list in the
+ * given order, exactly as the compositing loop does, and reports:
+ *   margin[p] the least relative distance of any decision quantity from its
+ *             threshold (|power| against the size of its terms; alpha against
+ *             min_alpha and 0.99; T against the cutoff), computed in double;
+ *   kind[p]   which decision that was: 1 power, 2 alpha floor, 3 cap,
+ *             4 cutoff (0 when the pixel evaluated nothing);
+ *   tie[p]    1 when a contributing entry shares its depth (bit-equal) with
+ *             another entry that would also contribute at the pixel, so their
+ *             order, the sort's tie-break, decides the result.
+ * Test infrastructure: the parity tests use it to show that every value off
+ * by more than the tolerance is a branch flip or a depth tie. */
+void pxo_pixel_decisions_f32(const pxs_projected_splat* projected, int32_t count,
+                             const pxs_camera* cam, const pxs_raster_options* opt,
+                             float* margin, int32_t* kind, int32_t* tie) {
+  const int width = cam->width, height = cam->height;
+  const size_t pixels = (size_t)width * (size_t)height;
+  if (pixels == 0) return;
+  const int cols = (width + 15) / 16, rows = (height + 15) / 16;
+  const int tiles = cols * rows;
+  int32_t* offsets = (int32_t*)malloc(sizeof(int32_t) * (size_t)(tiles + 1));
+  int64_t total = build_tiles_internal_f32(projected, count, width, height, offsets, NULL, 0);
+  int32_t* entries = (int32_t*)malloc(sizeof(int32_t) * (size_t)(total > 0 ? total : 1));
+  build_tiles_internal_f32(projected, count, width, height, offsets, entries, total);
+  const double floor_ = opt->min_alpha, cutoff = opt->transmittance_cutoff;
+  for (int ty = 0; ty < rows; ++ty) {
+    for (int tx = 0; tx < cols; ++tx) {
+      const int tile = ty * cols + tx;
+      const int begin = offsets[tile], end = offsets[tile + 1];
+      const int y_end = height < (ty + 1) * 16 ? height : (ty + 1) * 16;
+      const int x_end = width < (tx + 1) * 16 ? width : (tx + 1) * 16;
+      for (int y = ty * 16; y < y_end; ++y) {
+        for (int x = tx * 16; x < x_end; ++x) {
+          const size_t pixel = (size_t)y * (size_t)width + (size_t)x;
+          const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+          float T = 1.0f;
+          double best = INFINITY;
+          int best_kind = 0, tied = 0;
+          for (int e = begin; e < end; ++e) {
+            const pxs_projected_splat* s = &projected[entries[e]];
+            const float dx = px - s->mean[0], dy = py - s->mean[1];
+            const float power =
+                -0.5f * (s->conic[0] * dx * dx + s->conic[2] * dy * dy) - s->conic[1] * dx * dy;
+            const double size = 0.5 * fabs((double)s->conic[0] * dx * dx) +
+                                0.5 * fabs((double)s->conic[2] * dy * dy) +
+                                fabs((double)s->conic[1] * dx * dy) + 1e-30;
+            const double m_power = fabs((double)power) / size;
+            if (m_power < best) { best = m_power; best_kind = 1; }
+            if (power > 0.0f) continue;
+            const float raw = s->opacity * expf(power);
+            const double m_cap = fabs((double)raw - 0.99) / 0.99;
+            if (m_cap < best) { best = m_cap; best_kind = 3; }
+            const float alpha = raw < 0.99f ? raw : 0.99f;
+            const double m_floor = fabs((double)alpha - floor_) / floor_;
+            if (m_floor < best) { best = m_floor; best_kind = 2; }
+            if (alpha < opt->min_alpha) continue;
+            /* a contributing entry with another entry of its depth that would
+             * also pass both alpha tests here: their order is the tie-break,
+             * whichever of them the walk reaches first (the other may lie past
+             * the cutoff) */
+            if (!tied) {
+              for (int dir = -1; dir <= 1 && !tied; dir += 2) {
+                for (int f = e + dir; f >= begin && f < end; f += dir) {
+                  const pxs_projected_splat* o = &projected[entries[f]];
+                  if (memcmp(&o->depth, &s->depth, sizeof(float)) != 0) break;
+                  const float ox = px - o->mean[0], oy = py - o->mean[1];
+                  const float op = -0.5f * (o->conic[0] * ox * ox + o->conic[2] * oy * oy) -
+                                   o->conic[1] * ox * oy;
+                  if (op > 0.0f) continue;
+                  const float oraw = o->opacity * expf(op);
+                  if ((oraw < 0.99f ? oraw : 0.99f) >= opt->min_alpha) {
+                    tied = 1;
+                    break;
+                  }
+                }
+              }
+            }
+            T *= 1.0f - alpha;
+            const double m_cut = fabs((double)T - cutoff) / cutoff;
+            if (m_cut < best) { best = m_cut; best_kind = 4; }
+            if (T < opt->transmittance_cutoff) break;
+          }
+          if (margin) margin[pixel] = best_kind ? (float)best : INFINITY;
+          if (kind) kind[pixel] = best_kind;
+          if (tie) tie[pixel] = tied;
+        }
+      }
+    }
+  }
+  free(entries);
+  free(offsets);
+}

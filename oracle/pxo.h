@@ -119,6 +119,14 @@ int32_t pxo_densify_and_prune(float* params, int32_t n, int32_t rest_per_channel
 /* One Box-Muller normal from the reference's xorshift32 (SplatDensify.cpp:11-24). */
 float pxo_next_normal(uint32_t* state);
 
+/* Per-pixel decision margins of the compositing loop in the given list order
+ * (least relative distance of power, alpha and T from their thresholds, which
+ * decision it was, and whether two contributing entries share a depth); see
+ * pxo.c. */
+void pxo_pixel_decisions_f32(const pxs_projected_splat* projected, int32_t count,
+                             const pxs_camera* cam, const pxs_raster_options* opt,
+                             float* margin, int32_t* kind, int32_t* tie);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,16 +10,19 @@
 // converts between the component-major float arrays of pxs.h and the
 // reference's GaussianCloud / SplatView / SplatGradients types and calls the
 // reference's public functions.
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "parallax/io/ImageIo.h"
 #include "parallax/splat/SplatDensify.h"
 #include "parallax/splat/SplatRaster.h"
 #include "parallax/splat/SplatTrainer.h"
+#include "parallax/testing/SyntheticScene.h"
 #include "pxs.h"
 
 #ifdef PXREF_SHIM
@@ -199,6 +202,95 @@ struct RefTrainer {
   int rest = 0;
 };
 
+// A SplatBackend that renders, scores and differentiates a whole batch of
+// views per training step instead of the one view the trainer hands it. Each
+// view runs the reference's own CpuSplatBackend::renderAndAccumulate
+// (SplatTrainer.cpp:104-113) on its own host thread into its own
+// SplatGradients; the per-view gradients are then added in view order, which
+// is what the additive SplatGradients contract (SplatRaster.h:133-137) gives a
+// caller accumulating several views before one optimiser step. The trainer's
+// own applyGradients (SplatTrainer.cpp:218-256) then takes the Adam step.
+class BatchCpuBackend final : public SplatBackend {
+ public:
+  BatchCpuBackend(const std::vector<SplatTrainingView>* views, int threads)
+      : views_(views), threads_(std::max(1, threads)) {}
+
+  void setBatch(const int32_t* ids, int count) { batch_.assign(ids, ids + count); }
+
+  std::string name() const override { return "cpu-batch"; }
+
+  SplatImage render(const GaussianCloud& cloud, const SplatView& view,
+                    const RasterOptions& options) override {
+    return renderSplats(cloud, view, options);
+  }
+
+  float renderAndAccumulate(const GaussianCloud& cloud, const SplatView&,
+                            const RasterOptions& options, const std::vector<float>&,
+                            float ssim_weight, SplatGradients* gradients) override {
+    const size_t count = batch_.size();
+    const int stride = gradients->sh_rest_stride;
+    per_view_.resize(count);
+    losses_.assign(count, 0.f);
+    std::vector<std::thread> pool;
+    const int workers = static_cast<int>(std::min<size_t>(count, static_cast<size_t>(threads_)));
+    for (int w = 0; w < workers; ++w) {
+      pool.emplace_back([&, w] {
+        std::unique_ptr<SplatBackend> cpu = makeCpuSplatBackend();
+        for (size_t i = static_cast<size_t>(w); i < count; i += static_cast<size_t>(workers)) {
+          const SplatTrainingView& v = (*views_)[static_cast<size_t>(batch_[i])];
+          per_view_[i].resize(cloud.size(), stride);
+          losses_[i] = cpu->renderAndAccumulate(cloud, v.view, options, v.image, ssim_weight,
+                                                &per_view_[i]);
+        }
+      });
+    }
+    for (std::thread& t : pool) t.join();
+    pool.clear();
+    // gradients += sum over views, in view order, split by gaussian ranges
+    const size_t n = cloud.size();
+    const size_t chunk = (n + static_cast<size_t>(threads_) - 1) / static_cast<size_t>(threads_);
+    for (int w = 0; w < threads_; ++w) {
+      const size_t lo = std::min(n, static_cast<size_t>(w) * chunk);
+      const size_t hi = std::min(n, lo + chunk);
+      pool.emplace_back([&, lo, hi] {
+        for (size_t i = 0; i < count; ++i) {
+          const SplatGradients& g = per_view_[i];
+          for (size_t k = lo; k < hi; ++k) {
+            gradients->position[k] += g.position[k];
+            gradients->log_scale[k] += g.log_scale[k];
+            gradients->rotation[k] += g.rotation[k];
+            gradients->opacity_logit[k] += g.opacity_logit[k];
+            for (int c = 0; c < 3; ++c) gradients->dc[k][c] += g.dc[k][c];
+            for (int r = 0; r < stride; ++r)
+              gradients->sh_rest[k * static_cast<size_t>(stride) + static_cast<size_t>(r)] +=
+                  g.sh_rest[k * static_cast<size_t>(stride) + static_cast<size_t>(r)];
+            gradients->screen_gradient[k] += g.screen_gradient[k];
+            gradients->visible_count[k] += g.visible_count[k];
+          }
+        }
+      });
+    }
+    for (std::thread& t : pool) t.join();
+    float sum = 0.f;
+    for (float l : losses_) sum += l;
+    return count ? sum / static_cast<float>(count) : 0.f;
+  }
+
+ private:
+  const std::vector<SplatTrainingView>* views_;
+  int threads_;
+  std::vector<int32_t> batch_;
+  std::vector<SplatGradients> per_view_;
+  std::vector<float> losses_;
+};
+
+struct RefBatchTrainer {
+  std::vector<SplatTrainingView> views;
+  BatchCpuBackend* backend = nullptr;  // owned by trainer
+  std::unique_ptr<SplatTrainer> trainer;
+  int rest = 0;
+};
+
 }  // namespace
 
 extern "C" {
@@ -325,6 +417,37 @@ float ref_render_and_accumulate(const float* params, int n, int rest, int cloud_
   return loss;
 }
 
+// renderAndAccumulate's chain (SplatTrainer.cpp:104-113) on a projected list
+// the caller supplies, in the caller's order: rasterizeSplats, photometricLoss,
+// rasterizeSplatsBackward. projectSplats orders equal depths with the unstable
+// std::sort (SplatRaster.cpp:260-261); the parity tests pass its own output
+// re-sorted with equal depths by gaussian index, which gives the reference's
+// arithmetic under a specified tie order. `rgb` (may be null) gets the image.
+float ref_render_and_accumulate_projected(const float* params, int n, int rest, int cloud_sh,
+                                          const double* K, int width, int height,
+                                          const double* R, const double* t,
+                                          const pxs_raster_options* opt,
+                                          const pxs_projected_splat* projected, int count,
+                                          const float* target, float ssim_weight, float* rgb,
+                                          float* grads, float* screen, int32_t* visible) {
+  const GaussianCloud cloud = toCloud(params, n, rest, cloud_sh);
+  const SplatView view = toView(K, width, height, R, t);
+  const RasterOptions options = toOptions(opt);
+  std::vector<ProjectedSplat> p;
+  p.reserve(static_cast<size_t>(count));
+  for (int i = 0; i < count; ++i) p.push_back(fromProjected(projected[i]));
+  const SplatImage image = rasterizeSplats(p, view, options);
+  const size_t values = static_cast<size_t>(width) * height * 3;
+  if (rgb != nullptr) std::memcpy(rgb, image.rgb.data(), values * sizeof(float));
+  std::vector<float> tgt(target, target + values), dL;
+  const float loss = photometricLoss(image, tgt, ssim_weight, &dL);
+  SplatGradients g;
+  g.resize(cloud.size(), 3 * rest);
+  rasterizeSplatsBackward(cloud, view, options, p, image, dL, &g);
+  addGradients(g, rest, grads, screen, visible);
+  return loss;
+}
+
 // densifyAndPrune (SplatDensify.cpp:28-109). `params` has room for
 // config->max_gaussians gaussians; output stride is the new count.
 int ref_densify(float* params, int n, int rest, const float* screen, const int32_t* visible,
@@ -358,6 +481,93 @@ void* ref_trainer_create(const float* params, int n, int rest, int cloud_sh, int
 }
 
 void ref_trainer_destroy(void* handle) { delete static_cast<RefTrainer*>(handle); }
+
+// ------------------------------------------- the batched reference trainer
+//
+// The reference's SplatTrainer (its schedule and its Adam, applyGradients) with
+// BatchCpuBackend: each step renders, scores and differentiates the views set
+// by ref_batch_trainer_step on up to `threads` host threads, adds their
+// gradients, and takes one Adam step. This is the reference's CPU code for a
+// many-views-per-step training step.
+void* ref_batch_trainer_create(const float* params, int n, int rest, int cloud_sh,
+                               int n_views, const double* K, const int32_t* sizes,
+                               const double* R, const double* t, const float* const* images,
+                               const pxs_train_config* config, int threads) {
+  auto* holder = new RefBatchTrainer;
+  holder->rest = rest;
+  holder->views = toViews(n_views, K, sizes, R, t, images);
+  auto backend = std::make_unique<BatchCpuBackend>(&holder->views, threads);
+  holder->backend = backend.get();
+  // The trainer gets every camera (its scene extent, cameraExtent, comes from
+  // them) without the images; the view it picks each step is ignored by the
+  // backend, which renders the batch.
+  std::vector<SplatTrainingView> cameras;
+  for (const SplatTrainingView& v : holder->views) {
+    SplatTrainingView c;
+    c.view = v.view;
+    cameras.push_back(std::move(c));
+  }
+  holder->trainer = std::make_unique<SplatTrainer>(toCloud(params, n, rest, cloud_sh),
+                                                   std::move(cameras), toConfig(config),
+                                                   std::move(backend));
+  return holder;
+}
+
+// One training step over the `count` views `ids`; returns the trainer's
+// step() result and the mean loss over the batch.
+int ref_batch_trainer_step(void* handle, int count, const int32_t* ids, float* loss) {
+  auto* h = static_cast<RefBatchTrainer*>(handle);
+  h->backend->setBatch(ids, count);
+  const bool stepped = h->trainer->step();
+  if (loss != nullptr) *loss = h->trainer->lastLoss();
+  return stepped ? 1 : 0;
+}
+
+int ref_batch_trainer_download(void* handle, float* params, int capacity) {
+  auto* h = static_cast<RefBatchTrainer*>(handle);
+  return fromCloud(h->trainer->cloud(), h->rest, params, capacity);
+}
+
+void ref_batch_trainer_destroy(void* handle) { delete static_cast<RefBatchTrainer*>(handle); }
+
+// The benchmark clouds drawn with the reference's own generator,
+// parallax::testing::Rng (SyntheticScene.h:80-107): per gaussian, in this
+// order, position U[-1,1]^3, log sigma log_scale_mean + 0.5 N(0,1) per axis, a
+// quaternion normalise(N(0,1)^4) (w, x, y, z), opacity logit N(0,1), dc from an
+// RGB value 0.5 + 0.1 N(0,1) per channel, sh_rest 0.1 N(0,1). Component-major
+// output like every array of pxs.h.
+int ref_synthetic_cloud(uint64_t seed, int count, int rest, float log_scale_mean,
+                        float* params) {
+  if (count < 0 || params == nullptr) return -1;
+  parallax::testing::Rng rng(seed);
+  const size_t N = static_cast<size_t>(count);
+  const double c0 = 0.28209479177387814;
+  for (size_t g = 0; g < N; ++g) {
+    for (int a = 0; a < 3; ++a) params[(0 + a) * N + g] = static_cast<float>(rng.uniform(-1.0, 1.0));
+    for (int a = 0; a < 3; ++a)
+      params[(3 + a) * N + g] = static_cast<float>(log_scale_mean + 0.5 * rng.normal());
+    double q[4], norm = 0.0;
+    for (double& v : q) {
+      v = rng.normal();
+      norm += v * v;
+    }
+    norm = std::sqrt(norm);
+    if (norm < 1e-9) {
+      q[0] = 1.0;
+      q[1] = q[2] = q[3] = 0.0;
+      norm = 1.0;
+    }
+    for (int a = 0; a < 4; ++a) params[(6 + a) * N + g] = static_cast<float>(q[a] / norm);
+    params[10 * N + g] = static_cast<float>(rng.normal());
+    for (int c = 0; c < 3; ++c) {
+      const double rgb = 0.5 + 0.1 * rng.normal();
+      params[(11 + c) * N + g] = static_cast<float>((rgb - 0.5) / c0);
+    }
+    for (int k = 0; k < 3 * rest; ++k)
+      params[(14 + k) * N + g] = static_cast<float>(0.1 * rng.normal());
+  }
+  return 0;
+}
 
 int ref_trainer_step(void* handle) { return static_cast<RefTrainer*>(handle)->trainer->step(); }
 
@@ -472,6 +682,32 @@ void ref_config_defaults(pxs_train_config* c) {
   c->prune_scale_fraction = d.prune_scale_fraction;
   c->max_gaussians = d.max_gaussians;
   c->seed = d.seed;
+}
+
+// The training and raster settings of the multi-view benchmark step over the
+// reference's defaults (SplatTrainingConfig{}, RasterOptions{}): `sh_degree`
+// from the start, no densification, no opacity reset, `iterations` for the
+// position learning-rate schedule. Sizes let a caller allocate the structs
+// without declaring their layout.
+int ref_sizeof_train_config() { return static_cast<int>(sizeof(pxs_train_config)); }
+int ref_sizeof_raster_options() { return static_cast<int>(sizeof(pxs_raster_options)); }
+
+void ref_bench_settings(pxs_train_config* c, pxs_raster_options* o, int sh_degree,
+                        int iterations, int max_gaussians) {
+  ref_config_defaults(c);
+  c->iterations = iterations;
+  c->sh_degree = sh_degree;
+  c->sh_increase_interval = 0;
+  c->densify_from_iteration = 1000000000;
+  c->densify_until_iteration = 1000000000;
+  c->opacity_reset_interval = 0;
+  c->max_gaussians = max_gaussians;
+  const RasterOptions d;
+  for (int i = 0; i < 3; ++i) o->background[i] = d.background[i];
+  o->sh_degree = sh_degree;
+  o->min_alpha = d.min_alpha;
+  o->transmittance_cutoff = d.transmittance_cutoff;
+  o->screen_dilation = d.screen_dilation;
 }
 
 #ifdef PXREF_SHIM

@@ -68,6 +68,52 @@ def raster_case(name, sh_degree, count, width, height, seed, background=(0.0, 0.
     print(name, "visible", len(proj), "pairs", len(entries), "loss", loss)
 
 
+def ties_case():
+    """A cloud whose gaussians sit on 30 depth planes (camera along +z, so
+    every gaussian of a plane projects to a bit-equal depth), many of them
+    overlapping on screen. The reference orders equal depths with the unstable
+    std::sort (SplatRaster.cpp:260-261), so this fixture records its own
+    order as it comes out of projectSplats (`proj_*` unsorted), the tile lists
+    buildTiles' rule (SplatRaster.cpp:114-151) derives from that order, its
+    image, and, for the specified order (equal depths by gaussian index), the
+    reference's arithmetic on its own projections re-sorted that way: image,
+    loss and gradients."""
+    sh, count, width, height = 3, 900, 96, 72
+    params, rest = O.random_cloud(77, count, sh, log_scale_mean=-3.0)
+    rs = np.random.default_rng(5)
+    levels = rs.uniform(-0.6, 0.6, 30).astype(np.float32)
+    params[2] = levels[rs.integers(0, 30, count)]
+    params[0] = rs.uniform(-0.5, 0.5, count)
+    params[1] = rs.uniform(-0.4, 0.4, count)
+    # a few exact duplicates: fully coincident tied splats
+    params[:, 850:] = params[:, 800:850]
+    view = O.make_view(width, height, 2.5)
+    opt = RasterOptions(sh_degree=sh, background=(0.1, 0.2, 0.3))
+    proj = O.ref_project(params, rest, sh, view, opt)
+    offsets, entries = O.oracle_tiles(proj, width, height)
+    rgb, T = O.ref_render(params, rest, sh, view, opt)
+    rgb_from_list, _ = O.ref_rasterize(proj, view, opt)
+    assert np.array_equal(rgb, rgb_from_list)
+    target = np.random.default_rng(78).uniform(0, 1, rgb.shape).astype(np.float32)
+    ordered = O.tie_ordered(proj)
+    loss_i, rgb_i, grads_i, screen_i, visible_i = O.ref_render_and_accumulate_projected(
+        params, rest, sh, view, opt, ordered, target, 0.2)
+    d = proj["depth"].view(np.uint32)
+    runs = [(b, e) for b, e in O.tie_runs(d) if e - b > 1]
+    scrambled = sum(not np.all(np.diff(proj["index"][b:e]) > 0) for b, e in runs)
+    assert scrambled > 0, "the reference kept index order in every tie run"
+    np.savez_compressed(
+        os.path.join(HERE, "ties.npz"), params=params, rest=np.int32(rest),
+        cloud_sh_degree=np.int32(sh), **view_arrays(view), **options_arrays(opt),
+        **projected_arrays(proj), tile_offsets=offsets,
+        tile_entries=proj["index"][entries].astype(np.int32), rgb=rgb, transmittance=T,
+        target=target, ssim_weight=np.float32(0.2), index_order_rgb=rgb_i,
+        index_order_loss=np.float32(loss_i), index_order_grads=grads_i,
+        index_order_screen_gradient=screen_i, index_order_visible_count=visible_i)
+    print("ties: visible", len(proj), "tie runs", len(runs), "scrambled by std::sort", scrambled,
+          "pairs", len(entries))
+
+
 def densify_case():
     params, rest = O.random_cloud(21, 600, 1, log_scale_mean=-3.0)
     rs = np.random.default_rng(22)
@@ -122,9 +168,13 @@ def trainer_case():
 
 def main():
     O.build_oracle()
+    if sys.argv[1:] == ["ties"]:
+        ties_case()
+        return
     assert O.ref_available("ieee"), "oracle/_ref/libpxref_ieee.so is required"
     raster_case("raster_sh0", 0, 700, 64, 48, seed=31)
     raster_case("raster_sh3", 3, 500, 48, 40, seed=32, background=(0.2, 0.3, 0.4))
+    ties_case()
     densify_case()
     trainer_case()
 

@@ -85,6 +85,7 @@ def ref(kind: str = "ieee") -> ct.CDLL:
         lib.ref_photometric_loss.restype = ct.c_float
         lib.ref_mean_ssim.restype = ct.c_float
         lib.ref_render_and_accumulate.restype = ct.c_float
+        lib.ref_render_and_accumulate_projected.restype = ct.c_float
         lib.ref_densify.restype = ct.c_int
         lib.ref_trainer_create.restype = ct.c_void_p
         lib.ref_trainer_create.argtypes = [
@@ -390,6 +391,49 @@ def oracle_rasterize(projected, cam: Camera, opt: RasterOptions):
     return rgb, T
 
 
+def oracle_pixel_decisions(projected, cam: Camera, opt: RasterOptions):
+    """Per pixel, walking the list in `projected`'s order as the compositing loop
+    does: (margin, kind, tie). margin is the least relative distance of any
+    decision quantity (power, alpha against the floor and the 0.99 cap, T
+    against the cutoff) from its threshold; kind says which (1 power, 2 floor,
+    3 cap, 4 cutoff); tie is set where two contributing entries share a depth."""
+    proj = np.ascontiguousarray(projected)
+    n = cam.width * cam.height
+    margin = np.zeros(n, dtype=np.float32)
+    kind = np.zeros(n, dtype=np.int32)
+    tie = np.zeros(n, dtype=np.int32)
+    pxo().pxo_pixel_decisions_f32(as_ptr(proj), len(proj), ct.byref(cam), ct.byref(opt),
+                                  as_ptr(margin), as_ptr(kind), as_ptr(tie))
+    return margin, kind, tie.astype(bool)
+
+
+def relative_error(got, want, floor=1e-3):
+    """|got - want| / max(|want|, floor), elementwise."""
+    return np.abs(np.asarray(got, np.float64) - want) / np.maximum(np.abs(want), floor)
+
+
+def explain_image_differences(got, want, channels, margin, tie, rtol=1e-5, floor=1e-3,
+                              flip_margin=2e-5):
+    """Classifies every image value off by more than `rtol` (relative, with the
+    given floor). A value is explained when its pixel had a decision within
+    `flip_margin` of its threshold (a branch flip: the two sides' inputs differ
+    in the last bits) or two contributing entries at one depth (a depth tie,
+    whose order is the sort's tie-break). Returns a dict of counts; `unexplained`
+    must be 0."""
+    err = relative_error(got, want, floor).reshape(-1, channels)
+    bad_px = (err > rtol).any(axis=1)
+    flip = margin < flip_margin
+    return {"values": int(err.size), "beyond_tol": int((err > rtol).sum()),
+            "pixels_beyond_tol": int(bad_px.sum()),
+            "flip_pixels": int((bad_px & flip).sum()),
+            "tie_pixels": int((bad_px & ~flip & tie).sum()),
+            "unexplained": int((bad_px & ~flip & ~tie).sum()),
+            "candidate_flip_pixels": int(flip.sum()), "candidate_tie_pixels": int(tie.sum()),
+            "max_rel_err": float(err.max()) if err.size else 0.0,
+            "max_rel_err_explained_excluded":
+                float(err[~(flip | tie)].max()) if (~(flip | tie)).any() else 0.0}
+
+
 def oracle_loss(rendered, target, width, height, ssim_weight, want_grad=True):
     grad = np.zeros_like(rendered) if want_grad else None
     loss = pxo().pxo_photometric_loss_f32(as_ptr(rendered), as_ptr(target), width, height,
@@ -466,6 +510,91 @@ def ref_rasterize(projected, view: View, opt: RasterOptions, kind="ieee"):
     ref(kind).ref_rasterize(as_ptr(proj), len(proj), *view.ref_args(), ct.byref(opt),
                             as_ptr(rgb), as_ptr(T))
     return rgb, T
+
+
+def projected_from_fixture(d):
+    """The projected list a golden fixture stores as proj_* columns, in its
+    stored order."""
+    n = len(d["proj_index"])
+    p = np.zeros(n, dtype=PROJECTED_DTYPE)
+    for name in PROJECTED_DTYPE.names:
+        p[name] = d[f"proj_{name}"]
+    return p
+
+
+def tie_and_flip_pixels(orders, cam: Camera, opt: RasterOptions):
+    """(margin, tie) per pixel over several orders of one projected set: the
+    least decision margin and whether a depth tie decides the pixel in any of
+    them."""
+    margin, tie = None, None
+    for proj in orders:
+        m, _, t = oracle_pixel_decisions(proj, cam, opt)
+        margin = m if margin is None else np.minimum(margin, m)
+        tie = t if tie is None else (tie | t)
+    return margin, tie
+
+
+def tie_ordered(projected):
+    """A projected list re-sorted near to far with equal depths by gaussian
+    index: the order the device produces (the reference's std::sort leaves
+    equal depths in an unspecified order)."""
+    return np.sort(np.ascontiguousarray(projected), order=["depth", "index"], kind="stable")
+
+
+def ref_render_and_accumulate_projected(params, rest, sh_degree, view: View, opt: RasterOptions,
+                                        projected, target, ssim_weight, kind="ieee"):
+    """The reference's rasterizeSplats, photometricLoss and
+    rasterizeSplatsBackward on `projected` in its given order:
+    (loss, rgb, grads, screen_gradient, visible_count)."""
+    n = params.shape[1]
+    proj = np.ascontiguousarray(projected)
+    rgb = np.zeros(view.width * view.height * 3, dtype=np.float32)
+    grads = np.zeros_like(params)
+    screen = np.zeros(n, dtype=np.float32)
+    visible = np.zeros(n, dtype=np.int32)
+    loss = ref(kind).ref_render_and_accumulate_projected(
+        as_ptr(params), n, rest, sh_degree, *view.ref_args(), ct.byref(opt), as_ptr(proj),
+        len(proj), as_ptr(np.ascontiguousarray(target, dtype=np.float32)),
+        ct.c_float(ssim_weight), as_ptr(rgb), as_ptr(grads), as_ptr(screen), as_ptr(visible))
+    return loss, rgb, grads, screen, visible
+
+
+def tie_runs(depth_bits):
+    """[(begin, end)] of the runs of equal values in a sorted sequence."""
+    d = np.asarray(depth_bits)
+    if len(d) == 0:
+        return []
+    cuts = np.flatnonzero(d[1:] != d[:-1]) + 1
+    starts = np.concatenate([[0], cuts])
+    ends = np.concatenate([cuts, [len(d)]])
+    return list(zip(starts.tolist(), ends.tolist()))
+
+
+def lists_equal_up_to_ties(offsets, got, want, depth_of):
+    """Per-tile lists (flat gaussian ids cut by `offsets`) that hold the same
+    ids in the same order, except that within each run of equal depth inside a
+    tile the ids may come in any order. Returns (ok, runs, runs_reordered)."""
+    got = np.asarray(got)
+    want = np.asarray(want)
+    if got.shape != want.shape:
+        return False, 0, 0
+    if not np.array_equal(depth_of[got].view(np.uint32), depth_of[want].view(np.uint32)):
+        return False, 0, 0
+    runs = reordered = 0
+    for tile in range(len(offsets) - 1):
+        lo, hi = int(offsets[tile]), int(offsets[tile + 1])
+        dw = depth_of[want[lo:hi]].view(np.uint32)
+        for b, e in tie_runs(dw):
+            g, w = got[lo + b:lo + e], want[lo + b:lo + e]
+            if e - b > 1:
+                runs += 1
+                if not np.array_equal(g, w):
+                    reordered += 1
+                    if not np.array_equal(np.sort(g), np.sort(w)):
+                        return False, runs, reordered
+            elif g[0] != w[0]:
+                return False, runs, reordered
+    return True, runs, reordered
 
 
 def ref_loss(rendered, target, width, height, ssim_weight, kind="ieee"):

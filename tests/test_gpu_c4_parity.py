@@ -1,0 +1,138 @@
+"""Parity at the benchmarked configuration (C4: 1M gaussians, SH degree 3,
+1920x1440 views of a 64-camera pool, seeded).
+
+The device renders, scores and differentiates eight 480x360 windows of the
+first eight C4 views (the same cameras, principal point shifted; every window
+still projects and culls the whole 1M-gaussian cloud). The reference, compiled
+from its sources with IEEE arithmetic, does the same on the host:
+
+  * in its own order (projectSplats' unstable std::sort leaves equal depths in
+    an unspecified order; a uniform 1M cloud has tens of thousands of
+    bit-equal depths per view), the device image must differ only at pixels a
+    depth tie decides or where a decision sits within 2e-5 of its threshold
+    (a branch flip, bounded);
+  * in the specified order (its own projections re-sorted with equal depths by
+    gaussian index), the image must differ only by branch flips, the loss by
+    at most 1e-5 relative and the gradients by at most 1e-4 normwise per
+    parameter group, and the visible counts not at all.
+
+Every count (values beyond tolerance, flips, ties) is printed per window.
+"""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import parallax_b200 as px
+from parallax_b200._abi import RasterOptions
+from parallax_b200.scenes import crop_view, workload_scene
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_available("ieee"), reason="oracle/_ref not built")]
+
+RTOL, FLOOR, FLIP_MARGIN, FLIP_BOUND = 1e-5, 1e-3, 2e-5, 2e-2
+WINDOWS = [(0, 0), (1, 1), (2, 2), (3, 3), (0, 2), (1, 3), (2, 0), (3, 1)]
+GROUPS = {"position": slice(0, 3), "log_scale": slice(3, 6), "rotation": slice(6, 10),
+          "opacity": slice(10, 11), "dc": slice(11, 14), "sh_rest": slice(14, None)}
+
+
+def grad_errors(got, want):
+    return {name: float(np.linalg.norm(got[sl] - want[sl]) / max(np.linalg.norm(want[sl]), 1e-30))
+            for name, sl in GROUPS.items()}
+
+
+@pytest.fixture(scope="module")
+def c4_windows():
+    truth, start, views = workload_scene("c4")
+    opt = RasterOptions(sh_degree=3)
+    windows = []
+    for i, (cx, cy) in enumerate(WINDOWS):
+        v = views[i]
+        w, h = v.width // 4, v.height // 4
+        c = crop_view(v, cx * w, cy * h, w, h)
+        windows.append(O.View(tuple(c.K), c.width, c.height, np.asarray(c.R), np.asarray(c.t)))
+    # the reference's side of every window, on host threads
+    results = [None] * len(windows)
+
+    def reference(i):
+        view = windows[i]
+        cam = view.camera()
+        target, _ = O.ref_render(truth.params, truth.rest_per_channel, 3, view, opt)
+        own = O.ref_project(start.params, start.rest_per_channel, 3, view, opt)
+        rgb_own, _ = O.ref_rasterize(own, view, opt)
+        ordered = O.tie_ordered(own)
+        loss_i, rgb_i, g_i, s_i, v_i = O.ref_render_and_accumulate_projected(
+            start.params, start.rest_per_channel, 3, view, opt, ordered, target, 0.2)
+        margin, tie = O.tie_and_flip_pixels([own, ordered], cam, opt)
+        runs = sum(1 for b, e in O.tie_runs(own["depth"].view(np.uint32)) if e - b > 1)
+        results[i] = dict(target=target, rgb_own=rgb_own, loss_i=loss_i, rgb_i=rgb_i,
+                          grads_i=g_i, screen_i=s_i, visible_i=v_i, margin=margin, tie=tie,
+                          visible=len(own), tie_runs=runs)
+
+    threads = [threading.Thread(target=reference, args=(i,)) for i in range(len(windows))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert all(r is not None for r in results)
+    return start, opt, windows, results
+
+
+def check(got, want, channels, margin, tie, label):
+    ex = O.explain_image_differences(got, want, channels, margin, tie, RTOL, FLOOR, FLIP_MARGIN)
+    diff = np.abs(np.asarray(got, np.float64) - want).reshape(-1, channels).max(axis=1)
+    flip_only = (margin < FLIP_MARGIN) & ~tie
+    ex["max_abs_flip_change"] = float(diff[flip_only].max()) if flip_only.any() else 0.0
+    print(label, ex)
+    assert ex["unexplained"] == 0, (label, ex)
+    assert ex["max_abs_flip_change"] <= FLIP_BOUND, (label, ex)
+    return ex
+
+
+def test_c4_window_images_match_the_reference(ctx_c4, c4_windows):
+    start, opt, windows, results = c4_windows
+    totals = {"tie_pixels": 0, "flip_pixels": 0, "beyond_tol": 0, "values": 0}
+    for i, (view, r) in enumerate(zip(windows, results)):
+        rgb, _ = px.render_splats(start, view.camera(), opt, ctx_c4)
+        ex = check(rgb, r["rgb_own"], 3, r["margin"], r["tie"],
+                   f"window {i} vs reference order ({r['visible']} visible, "
+                   f"{r['tie_runs']} equal-depth runs)")
+        for k in totals:
+            totals[k] += ex[k]
+        no_tie = np.zeros_like(r["tie"])
+        check(rgb, r["rgb_i"], 3, r["margin"], no_tie, f"window {i} vs index order")
+    print("C4 windows, device vs reference's own order:", totals)
+
+
+def test_c4_window_loss_and_gradients_match_the_reference(ctx_c4, c4_windows):
+    start, opt, windows, results = c4_windows
+    worst = {}
+    for i, (view, r) in enumerate(zip(windows, results)):
+        grads = px.SplatGradients.zeros(start)
+        loss = px.render_and_accumulate(start, view.camera(), opt, r["target"], 0.2, grads,
+                                        ctx_c4)
+        rel = abs(loss - r["loss_i"]) / abs(r["loss_i"])
+        errs = grad_errors(grads.params, r["grads_i"])
+        screen = float(np.linalg.norm(grads.screen_gradient - r["screen_i"])
+                       / max(np.linalg.norm(r["screen_i"]), 1e-30))
+        print(f"window {i}: loss {loss:.7f} (reference {r['loss_i']:.7f}, rel {rel:.2e}); "
+              f"gradient errors {errs}; screen gradient {screen:.2e}")
+        assert rel <= 1e-5, (i, rel)
+        assert np.array_equal(grads.visible_count, r["visible_i"]), i
+        assert max(errs.values()) <= 1e-4, (i, errs)
+        assert screen <= 1e-4, (i, screen)
+        for k, v in errs.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    print("C4 windows, worst gradient error per group:", worst)
+
+
+@pytest.fixture(scope="module")
+def ctx_c4():
+    available, _, reason = px.splat_gpu_availability()
+    assert available, reason
+    c = px.Context(0)
+    yield c
+    c.close()

@@ -235,3 +235,52 @@ def test_f64_oracle_gradient_matches_central_differences():
             scale = max(abs(numeric), abs(grads[c, g]), 1e-3)
             worst = max(worst, abs(numeric - grads[c, g]) / scale)
     assert worst < 1e-5
+
+
+def test_tie_fixture_holds_the_references_own_scrambled_order():
+    """tests/golden/ties.npz: 900 gaussians on 30 depth planes. The reference's
+    std::sort leaves each run of equal depths in an unspecified order; the
+    fixture keeps that order as it came out of projectSplats."""
+    d = load("ties.npz")
+    proj = golden_projected(d)
+    runs = [(b, e) for b, e in O.tie_runs(proj["depth"].view(np.uint32)) if e - b > 1]
+    assert len(runs) == 30
+    assert sum(not np.all(np.diff(proj["index"][b:e]) > 0) for b, e in runs) == 30
+    # the oracle sorts equal depths by gaussian index: the same splats, bit for
+    # bit, in the specified order
+    view, opt = golden_view(d), golden_options(d)
+    ora = O.oracle_project(d["params"], int(d["rest"]), int(d["cloud_sh_degree"]),
+                           view.camera(), opt)
+    ordered = O.tie_ordered(proj)
+    for name in ora.dtype.names:
+        assert np.array_equal(np.ascontiguousarray(ora[name]).view(np.uint8),
+                              np.ascontiguousarray(ordered[name]).view(np.uint8)), name
+
+
+def test_tie_fixture_lists_and_image_differ_from_the_index_order_only_at_ties():
+    d = load("ties.npz")
+    view, opt = golden_view(d), golden_options(d)
+    cam = view.camera()
+    proj = golden_projected(d)
+    ordered = O.tie_ordered(proj)
+    offsets, entries = O.oracle_tiles(ordered, view.width, view.height)
+    assert np.array_equal(offsets, d["tile_offsets"])
+    depth_of = np.zeros(d["params"].shape[1], dtype=np.float32)
+    depth_of[proj["index"]] = proj["depth"]
+    ok, runs, reordered = O.lists_equal_up_to_ties(offsets, ordered["index"][entries],
+                                                    d["tile_entries"], depth_of)
+    assert ok and runs > 0 and reordered > 0, (runs, reordered)
+    # the index-order image (the oracle) against the reference's own image:
+    # every value off by more than 1e-5 is at a pixel that a depth tie decides
+    rgb, _ = O.oracle_rasterize(ordered, cam, opt)
+    assert np.array_equal(bits(rgb), bits(d["index_order_rgb"]))
+    margin, tie = O.tie_and_flip_pixels([proj, ordered], cam, opt)
+    ex = O.explain_image_differences(rgb, d["rgb"], 3, np.full_like(margin, np.inf), tie)
+    assert ex["unexplained"] == 0, ex
+    assert ex["tie_pixels"] > 0, ex  # the tie order changes the image
+    # the oracle's gradient in the index order is the reference's arithmetic
+    loss, g, s, v = O.oracle_render_and_accumulate(
+        d["params"], int(d["rest"]), int(d["cloud_sh_degree"]), cam, opt, d["target"], 0.2)
+    assert np.float32(loss) == d["index_order_loss"]
+    assert np.array_equal(bits(g), bits(d["index_order_grads"]))
+    assert np.array_equal(v, d["index_order_visible_count"])
