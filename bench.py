@@ -4,9 +4,10 @@
 Workload (default "c4"): 1M gaussians, SH degree 3, a 64-camera pool at
 1920x1440 (Fibonacci sphere, radius 3, 60 degree FOV), 8 views per step
 rendered, differentiated and accumulated, then one Adam step. Synthetic data:
-truth cloud seed 1 (targets rendered from it), start cloud seed 2, cameras
-seed 3; inputs are larger than L2 (1M gaussians x 236 B of parameters, 8 x 33 MB
-of targets per step), so no L2 flush is needed between steps.
+truth cloud seed 1 (targets rendered from it and quantised to 8-bit frames),
+start cloud seed 2, cameras seed 3; inputs are larger than L2 (1M gaussians x
+236 B of parameters, 8 x 33 MB of targets per step), so no L2 flush is needed
+between steps.
 
 Arms:
   ours (default)  the batched, CUDA-graph-captured step; also the plain
@@ -14,15 +15,21 @@ Arms:
                   step's 8-bit target frames copied from pinned host memory and
                   converted on the device (and, beside it, FP32 images), per-stage
                   device timing, the roofline of the dominant kernel and, on
-                  rank 0 at N=1, the reference CPU trainer's rate on a bounded
-                  sample.
-  reference       the reference's own CPU implementation (compiled from its
-                  sources into oracle/_ref with its release flags) on a bounded
-                  sample of the same workload, one view per host thread.
+                  rank 0 at N=1, one full step of the reference's CPU trainer.
+  reference       the reference's own CPU trainer (compiled from its sources into
+                  oracle/_ref with its release flags) on the same workload and
+                  view schedule: every step renders, scores and differentiates
+                  the step's views, one view per host thread, adds the
+                  gradients and takes the reference's Adam step
+                  (oracle/ref_bench.py). It never loads the product library.
 
-Multi-GPU (torchrun): data parallel over views; each rank renders and
-differentiates its own 8 views per step (weak scaling), the gradients are summed
-with an NCCL all-reduce, every rank applies the same Adam step.
+Multi-GPU: `--gpus N` starts N ranks itself (one process per GPU, RANK /
+LOCAL_RANK / WORLD_SIZE / MASTER_ADDR=127.0.0.1 in their environment) unless
+a launcher (torchrun) already set WORLD_SIZE. Data parallel over views: each
+rank renders and differentiates its own 8 views per step (weak scaling), the
+gradient block is summed with one NCCL all-reduce, and every rank applies the
+same Adam step. `--dry-run` runs the same launch and rank protocol on CPU
+(gloo) without a device, for tests.
 """
 from __future__ import annotations
 
@@ -43,6 +50,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STAGES = ["project", "bin", "forward", "loss", "backward", "param_grads", "adam"]
+DATA = ("synthetic (seeded: truth cloud 1, start cloud 2, cameras 3; targets rendered from the "
+        "truth cloud, quantised to 8-bit frames)")
 METRIC = "train steps/s (fwd+bwd+Adam, 8 views of 1920x1440, 1M gaussians SH3), batched graph-captured step"
 
 
@@ -64,7 +73,69 @@ def parse_args():
     p.add_argument("--px", default="",
                    help="pixels per thread 'F,B' for compositing and its adjoint "
                         "(default: the autotuner picks)")
+    p.add_argument("--dry-run", action="store_true",
+                   help="launch and rank protocol only, on CPU over gloo (no device)")
     return p.parse_args()
+
+
+# The benchmark workloads; "c4" is the headline. They equal
+# parallax_b200.scenes.WORKLOADS (tests/test_bench_names.py), restated here so
+# the reference arm never imports the product package.
+BENCH_WORKLOADS = {
+    "c4": dict(gaussians=1_000_000, sh_degree=3, views_per_step=8, pool=64, width=1920,
+               height=1440, layout=0),
+}
+
+
+def workload_config(name, w, V, pool):
+    """The `config` of the JSON line; both arms print the same one."""
+    return {"workload": f"{name}: {w['gaussians']} gaussians SH{w['sh_degree']}, {V} views/step "
+                        f"at {w['width']}x{w['height']} from a {pool}-camera pool, "
+                        "fwd+L1/SSIM+bwd+Adam",
+            "gaussians": w["gaussians"], "sh_degree": w["sh_degree"], "views_per_step": V,
+            "pool": pool, "width": w["width"], "height": w["height"],
+            "l2": "inputs larger than L2 (no flush)"}
+
+
+def view_ids(step, V, pool, rank=0):
+    """The views of `step` on `rank`: V consecutive cameras of the pool."""
+    base = (step * V + rank * 7) % pool
+    return [(base + i) % pool for i in range(V)]
+
+
+def free_port():
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def spawn_ranks(args) -> int:
+    """Starts args.gpus ranks of this script (one per GPU) and waits for them.
+    Rank 0 prints the JSON line. If a rank fails, the others get the process
+    group's timeout to end on their own, then are stopped."""
+    port = free_port()
+    procs = []
+    for r in range(args.gpus):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(args.gpus),
+                   LOCAL_WORLD_SIZE=str(args.gpus), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:],
+                                      env=env))
+    rc, failed_at = 0, None
+    while any(p.poll() is None for p in procs):
+        for p in procs:
+            if p.poll() not in (None, 0) and failed_at is None:
+                failed_at = time.time()
+        if failed_at is not None and time.time() - failed_at > 240:
+            for p in procs:
+                if p.poll() is None:
+                    p.kill()
+        time.sleep(0.2)
+    for p in procs:
+        rc = rc or p.returncode
+    return rc
 
 
 def dist_env():
@@ -122,158 +193,29 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-# ------------------------------------------------- reference CPU sample
-
-CROPS = [(0, 0), (1, 1), (2, 2), (3, 3), (0, 2), (1, 3), (2, 0), (3, 1)]
+# ------------------------------------------------------ reference CPU trainer
 
 
-def load_cpu_baseline():
-    """The reference compiled from its sources with its own release flags, or
-    the C restatement when that build is absent. Returns (kind, lib)."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "libpxref_fast.so")
-    if os.path.exists(ref):
-        lib = ct.CDLL(ref)
-        view = [_vp, ct.c_int, ct.c_int, ct.c_int, _vp, ct.c_int, ct.c_int, _vp, _vp, _vp]
-        _sig(lib.ref_project, ct.c_int, view + [_vp])
-        _sig(lib.ref_render, None, view + [_vp, _vp])
-        _sig(lib.ref_render_and_accumulate, ct.c_float,
-             view + [_vp, ct.c_float, _vp, _vp, _vp])
-        return "reference", lib
-    port = os.path.join(ROOT, "oracle", "libpxo.so")
-    if not os.path.exists(port):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
-    lib = ct.CDLL(port)
-    i32 = ct.c_int32
-    _sig(lib.pxo_project_f32, i32, [_vp, i32, i32, i32, _vp, _vp, _vp])
-    _sig(lib.pxo_rasterize_f32, None, [_vp, i32, _vp, _vp, _vp, _vp])
-    _sig(lib.pxo_render_and_accumulate_f32, ct.c_float,
-         [_vp, i32, i32, i32, _vp, _vp, _vp, ct.c_float, _vp, _vp, _vp])
-    return "port", lib
+def reference_step(workload, V, pool, threads, steps_needed):
+    """The reference's own CPU trainer on the workload (oracle/ref_bench.py),
+    with targets rendered for the views of the first `steps_needed` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_bench
+
+    w = BENCH_WORKLOADS[workload]
+    needed = sorted({i for s in range(steps_needed) for i in view_ids(s, V, pool)})
+    return ref_bench.ReferenceBatchStep(
+        w["gaussians"], w["sh_degree"], pool, w["width"], w["height"], threads,
+        target_views=needed, log=lambda m: print(m, file=sys.stderr, flush=True))
 
 
-_vp = ct.c_void_p
-
-
-def _sig(fn, restype, argtypes):
-    fn.restype = restype
-    fn.argtypes = argtypes
-
-
-class CpuSample:
-    """One view per host thread: the reference's projectSplats over the full
-    view, then renderAndAccumulate (project, rasterise, L1+SSIM, backward) on a
-    1/16 window of it. A full view's cost is estimated as
-    t(project full) + 16 * (t(renderAndAccumulate window) - t(project window)):
-    compositing, loss and backward scale with pixels, projection does not."""
-
-    def __init__(self, truth, start, views, kind, lib, threads):
-        from parallax_b200.scenes import crop_view
-
-        self.kind, self.lib = kind, lib
-        self.start = start
-        self.views = views[:8]
-        self.threads = threads
-        self.jobs = []
-        w, h = self.views[0].width // 4, self.views[0].height // 4
-        for i, view in enumerate(self.views):
-            cx, cy = CROPS[i % len(CROPS)]
-            crop = crop_view(view, cx * w, cy * h, w, h)
-            target = self.render(truth, crop)  # the reference renders its own targets
-            self.jobs.append((view, crop, target))
-
-    def _view_args(self, v):
-        K = np.array(v.K, dtype=np.float64)
-        R = np.ascontiguousarray(np.asarray(v.R, dtype=np.float64).reshape(9))
-        t = np.ascontiguousarray(np.asarray(v.t, dtype=np.float64).reshape(3))
-        return (K, R, t)
-
-    def render(self, cloud, view):
-        rgb = np.zeros(view.width * view.height * 3, dtype=np.float32)
-        if self.kind == "reference":
-            K, R, t = self._view_args(view)
-            self.lib.ref_render(cloud.params.ctypes.data, cloud.count, cloud.rest_per_channel,
-                                cloud.sh_degree, K.ctypes.data, view.width, view.height,
-                                R.ctypes.data, t.ctypes.data, ct.byref(self.options()),
-                                rgb.ctypes.data, None)
-        else:
-            cam = view.camera()
-            proj = np.zeros(cloud.count * 64 + 64, dtype=np.uint8)
-            n = self.lib.pxo_project_f32(cloud.params.ctypes.data, cloud.count,
-                                         cloud.rest_per_channel, cloud.sh_degree, ct.byref(cam),
-                                         ct.byref(self.options()), proj.ctypes.data)
-            self.lib.pxo_rasterize_f32(proj.ctypes.data, n, ct.byref(cam),
-                                       ct.byref(self.options()), rgb.ctypes.data, None)
-        return rgb
-
-    def options(self):
-        from parallax_b200 import RasterOptions
-        return RasterOptions(sh_degree=3)
-
-    def project(self, view):
-        c = self.start
-        out = np.zeros(c.count * 64 + 64, dtype=np.uint8)
-        if self.kind == "reference":
-            K, R, t = self._view_args(view)
-            self.lib.ref_project(c.params.ctypes.data, c.count, c.rest_per_channel, c.sh_degree,
-                                 K.ctypes.data, view.width, view.height, R.ctypes.data,
-                                 t.ctypes.data, ct.byref(self.options()), out.ctypes.data)
-        else:
-            cam = view.camera()
-            self.lib.pxo_project_f32(c.params.ctypes.data, c.count, c.rest_per_channel,
-                                     c.sh_degree, ct.byref(cam), ct.byref(self.options()),
-                                     out.ctypes.data)
-
-    def render_and_accumulate(self, view, target):
-        c = self.start
-        grads = np.zeros_like(c.params)
-        screen = np.zeros(c.count, dtype=np.float32)
-        visible = np.zeros(c.count, dtype=np.int32)
-        if self.kind == "reference":
-            K, R, t = self._view_args(view)
-            self.lib.ref_render_and_accumulate(
-                c.params.ctypes.data, c.count, c.rest_per_channel, c.sh_degree, K.ctypes.data,
-                view.width, view.height, R.ctypes.data, t.ctypes.data, ct.byref(self.options()),
-                target.ctypes.data, ct.c_float(0.2), grads.ctypes.data, screen.ctypes.data,
-                visible.ctypes.data)
-        else:
-            cam = view.camera()
-            self.lib.pxo_render_and_accumulate_f32(
-                c.params.ctypes.data, c.count, c.rest_per_channel, c.sh_degree, ct.byref(cam),
-                ct.byref(self.options()), target.ctypes.data, ct.c_float(0.2),
-                grads.ctypes.data, screen.ctypes.data, visible.ctypes.data)
-
-    def run(self):
-        """Estimated seconds for one full step (8 views) on `threads` threads."""
-        estimates = [0.0] * len(self.jobs)
-
-        def work(i):
-            view, crop, target = self.jobs[i]
-            t0 = time.perf_counter()
-            self.project(view)
-            t1 = time.perf_counter()
-            self.project(crop)
-            t2 = time.perf_counter()
-            self.render_and_accumulate(crop, target)
-            t3 = time.perf_counter()
-            estimates[i] = (t1 - t0) + 16.0 * max(0.0, (t3 - t2) - (t2 - t1))
-
-        pending = list(range(len(self.jobs)))
-        while pending:
-            batch, pending = pending[: self.threads], pending[self.threads:]
-            ts = [threading.Thread(target=work, args=(i,)) for i in batch]
-            for t in ts:
-                t.start()
-            for t in ts:
-                t.join()
-        return sum(estimates) / min(self.threads, len(self.jobs))
-
-    def describe(self):
-        v = self.views[0]
-        return (f"{len(self.jobs)} views, one per thread: the reference's projectSplats over the "
-                f"full {v.width}x{v.height} view plus renderAndAccumulate on a "
-                f"{v.width // 4}x{v.height // 4} window (1/16 of the pixels); a view costs "
-                f"t(project) + 16 x t(window fwd+loss+bwd); step = sum over 8 views / threads; "
-                f"1M gaussians SH3, {self.kind} build")
+def reference_sample(w, V, threads):
+    return (f"whole steps of the reference's CPU trainer (oracle/_ref/libpxref_fast.so, its "
+            f"-O3 -ffast-math release flags): per step {V} views of {w['width']}x{w['height']}, "
+            f"each projectSplats + rasterizeSplats + photometricLoss + rasterizeSplatsBackward "
+            f"(CpuSplatBackend::renderAndAccumulate) on its own host thread ({threads} threads), "
+            f"gradients added, then SplatTrainer's own Adam step over {w['gaussians']} gaussians "
+            f"SH{w['sh_degree']}; nothing extrapolated")
 
 
 # ------------------------------------------------------------ our arm
@@ -354,8 +296,7 @@ def run_ours(args):
     pool = len(views)
 
     def ids_for(step):
-        base = (step * V + rank * 7) % pool
-        return [(base + i) % pool for i in range(V)]
+        return view_ids(step, V, pool, rank)
 
     if world > 1:
         # data parallel over views: each rank renders its own V views, the
@@ -512,15 +453,19 @@ def run_ours(args):
                      "frac": t_roof * 1e3 / ms_batched}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload in BENCH_WORKLOADS:
+        # one whole step of the reference's CPU trainer on this workload: a
+        # bounded sample (about half a minute on the host cores)
         try:
-            kind, clib = load_cpu_baseline()
-            threads = min(8, os.cpu_count() or 1)
-            sample = CpuSample(truth, start, views, kind, clib, threads)
-            seconds = sample.run()
-            cpu = {"value": 1.0 / seconds, "unit": "steps/s", "cores": threads, "kind": kind,
-                   "sample": sample.describe(), "seconds_per_step_estimate": seconds,
-                   "host_cores": os.cpu_count()}
+            threads = min(V, os.cpu_count() or 1)
+            ref = reference_step(args.workload, V, pool, threads, 1)
+            t0 = time.perf_counter()
+            ref.step(view_ids(0, V, pool))
+            seconds = time.perf_counter() - t0
+            ref.close()
+            cpu = {"value": 1.0 / seconds, "unit": "steps/s", "cores": threads,
+                   "kind": "reference", "sample": "one " + reference_sample(w, V, threads)[6:],
+                   "seconds_per_step": seconds, "host_cores": os.cpu_count()}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "unavailable",
                    "sample": f"failed: {exc}"}
@@ -537,15 +482,10 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "fp32",
-        "data": "synthetic (seeded: truth cloud 1, start cloud 2, cameras 3; targets rendered "
-                "from the truth cloud, quantised to 8-bit frames)",
-        "config": {"workload": f"{args.workload}: {N} gaussians SH{w['sh_degree']}, "
-                               f"{V} views/step at {w['width']}x{w['height']} from a {pool}-camera "
-                               "pool, fwd+L1/SSIM+bwd+Adam",
-                   "gaussians": N, "views_per_step": V, "width": w["width"],
-                   "height": w["height"], "parallelism": f"dp{world} over views",
-                   "l2": "inputs larger than L2 (no flush)",
-                   "pixels_per_thread": {"forward": fpx.value, "backward": bpx.value}},
+        "data": DATA,
+        "config": workload_config(args.workload, w, V, pool),
+        "parallelism": f"dp{world} over views, one GPU per rank",
+        "tuning": {"pixels_per_thread": {"forward": fpx.value, "backward": bpx.value}},
         "plain": {"ms_per_step": ms_plain,
                   "value": world * 1000.0 / ms_plain if ms_plain else None,
                   "batched_over_plain": (ms_plain / ms_batched) if ms_plain else None,
@@ -666,34 +606,40 @@ def traffic_from_profiles(kernel):
 
 
 def run_reference(args):
+    """The reference's CPU trainer on the workload and view schedule of our arm
+    (rank 0 only; other ranks exit at once). Never imports the product."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
-    import parallax_b200 as px  # host-side scene generation only
-    from parallax_b200.scenes import WORKLOADS, orbit_views
-
-    w = WORKLOADS[args.workload]
-    try:
-        kind, clib = load_cpu_baseline()
-    except Exception as exc:
-        print(json.dumps({"impl": "reference", "unavailable": f"no CPU build: {exc}"}))
+    n_gpus = world if "WORLD_SIZE" in os.environ else args.gpus
+    if args.workload not in BENCH_WORKLOADS:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": f"no reference arm for workload {args.workload}"}))
         return
-    truth = px.synthetic_cloud(1, w["gaussians"], w["sh_degree"])
-    start = px.synthetic_cloud(2, w["gaussians"], w["sh_degree"])
-    views = orbit_views(3, w["pool"], w["width"], w["height"], layout=w["layout"])
-    threads = min(8, os.cpu_count() or 1)
-    sample = CpuSample(truth, start, views, kind, clib, threads)
-    for _ in range(args.warmup):
-        sample.run()
-    times = [sample.run() for _ in range(args.steps)]
-    seconds = statistics.median(times)
+    w = BENCH_WORKLOADS[args.workload]
+    V = args.views or w["views_per_step"]
+    pool = args.pool or w["pool"]
+    threads = min(V, os.cpu_count() or 1)
+    try:
+        ref = reference_step(args.workload, V, pool, threads, args.warmup + args.steps)
+    except Exception as exc:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build: {exc}"}))
+        return
+    for s in range(args.warmup):
+        ref.step(view_ids(s, V, pool))
+        print(f"reference warm-up step {s + 1}/{args.warmup}", file=sys.stderr, flush=True)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        ref.step(view_ids(args.warmup + s, V, pool))
+    seconds = (time.perf_counter() - t0) / max(args.steps, 1)
+    ref.close()
     value = 1.0 / seconds
     line = {
         "impl": "reference",
         "metric": METRIC,
         "value": value,
         "unit": "steps/s",
-        "n_gpus": world,
+        "n_gpus": n_gpus,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": seconds * 1e3,
@@ -701,22 +647,51 @@ def run_reference(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "fp32",
-        "data": "synthetic (seeded, same scene as ours; targets rendered by the reference)",
-        "config": {"workload": f"{args.workload}: {w['gaussians']} gaussians SH{w['sh_degree']}, "
-                               f"{w['views_per_step']} views/step at {w['width']}x{w['height']}",
-                   "parallelism": "host threads, one view each"},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": kind,
-                         "sample": sample.describe()},
+        "data": DATA,
+        "config": workload_config(args.workload, w, V, pool),
+        "parallelism": f"host threads, one view each ({threads} threads)",
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads,
+                         "kind": "reference", "sample": reference_sample(w, V, threads),
+                         "host_cores": os.cpu_count()},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "final_loss": ref.loss,
     }
     print(json.dumps(line))
+
+
+def run_dry(args):
+    """The launch and rank protocol of the multi-GPU run without a device:
+    every rank joins a gloo group, reports, and the ranks agree on a maximum
+    time the way the timed region does."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    print(f"rank {rank} of {world} started (local rank {local})", file=sys.stderr, flush=True)
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    t = torch.tensor([float(rank + 1)])
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": "steps/s", "n_gpus": world,
+                          "dry_run": True, "max_over_ranks": float(t.item())}))
 
 
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
+    if args.dry_run:
+        run_dry(args)
     elif args.workload == "c5":
         run_multi_scene(args)
     else:
