@@ -273,7 +273,11 @@ int pxs_adam_device(pxs_context* context, float* params, float* grads, float* m,
  * PXS_ERR_INVALID. The call allocates no device memory and calls no
  * allocating routine. The first call on each device (the current one) looks
  * up the array's address and sets the kernel's shared-memory limit, once; make
- * that first call before any stream capture. Every call on a device shares
+ * that first call before any stream capture. On a thread with no current
+ * context that first call also creates the device's primary context and loads
+ * this library's kernels, which takes device memory of its own (as any first
+ * CUDA call does); a caller whose allocator owns the device's memory should
+ * make it, or create the context, before setting its memory budget. Every call on a device shares
  * the one array: calls whose work overlaps on the GPU (two streams, two host
  * threads) race and give wrong results, so order them (one stream, or
  * events). Each call clears the sums it uses before the kernel runs.
