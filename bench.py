@@ -390,13 +390,49 @@ def run_ours(args):
 
     e2e = None
     if not args.no_e2e:
-        # each step's 8-bit frames cross from pinned host memory and are
-        # converted on the device (pxs_trainer_ingest_images), then the step
-        # runs and its loss is read back
-        def e2e_step(_):
+        def stage(ids):
+            id_arr = (ct.c_int32 * len(ids))(*ids)
+            ptrs = (ct.c_void_p * len(ids))(*[frames[i].data_ptr() for i in ids])
+            ws = (ct.c_int32 * len(ids))(*[views[i].width for i in ids])
+            hs = (ct.c_int32 * len(ids))(*[views[i].height for i in ids])
+            trainer._check(lib.pxs_trainer_stage_images(trainer.handle, len(ids), id_arr, ptrs,
+                                                        ws, hs))
+
+        # The feeding loop of a training job: every step's 8-bit frames cross
+        # from pinned host memory, staged one step ahead so the copy overlaps
+        # the step before (pxs_trainer_stage_images), are converted on the
+        # device, the step runs and its loss is read back. Exactly `steps`
+        # frame sets are copied inside the timed region, one per step.
+        def timed_e2e(steps):
+            barrier()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            first = step_counter[0] + 1
+            stage(ids_for(first))
+            for k in range(steps):
+                if k + 1 < steps:
+                    stage(ids_for(first + k + 1))
+                batch_step(first + k)  # reads the loss back to the host
+            step_counter[0] = first + steps - 1
+            b.record(stream)
+            b.synchronize()
+            torch.cuda.synchronize()
+            barrier()
+            ms = a.elapsed_time(b) / steps
+            if world > 1:
+                import torch.distributed as dist
+                t = torch.tensor([ms], device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
+            return ms
+
+        # the same without overlap: ingest (synchronous), then the step
+        def e2e_serial_step(_):
             step_counter[0] += 1
             ingest(ids_for(step_counter[0]))
-            batch_step(step_counter[0])  # reads the loss back to the host
+            batch_step(step_counter[0])
 
         # the same with the targets uploaded as FP32 images (pxs_trainer_set_images)
         def e2e_float_step(_):
@@ -407,16 +443,22 @@ def run_ours(args):
             trainer._check(lib.pxs_trainer_set_images(trainer.handle, V, id_arr, ptrs))
             batch_step(step_counter[0])
 
-        e2e_step(0)
-        ms_e2e = timed(e2e_step, args.steps)
+        timed_e2e(2)  # warm the staging buffers and the graph
+        ms_e2e = timed_e2e(args.steps)
         h2d = sum(views[i].width * views[i].height * 3 for i in ids_for(0))
+        e2e_serial_step(0)
+        ms_e2e_serial = timed(e2e_serial_step, args.steps)
         e2e_float_step(0)
         ms_e2e_float = timed(e2e_float_step, args.steps)
         # restore the 8-bit targets of the views the float leg replaced
         ingest(list(range(len(views))))
         e2e = {"value": world * 1000.0 / ms_e2e, "unit": "steps/s", "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 + 4,
-               "inputs": "8-bit RGB frames at the view size, converted on the device",
+               "inputs": "8-bit RGB frames at the view size from pinned host memory, staged "
+                         "one step ahead on a copy stream and converted on the device",
+               "serial": {"value": world * 1000.0 / ms_e2e_serial,
+                          "ms_per_step": ms_e2e_serial, "h2d_bytes_per_step": h2d,
+                          "inputs": "the same frames ingested synchronously before each step"},
                "fp32_targets": {"value": world * 1000.0 / ms_e2e_float,
                                 "ms_per_step": ms_e2e_float, "h2d_bytes_per_step": 4 * h2d,
                                 "inputs": "FP32 RGB images (pxs_trainer_set_images)"}}

@@ -344,21 +344,28 @@ int pxs_trainer_create_scenes(const pxs_train_config* config, const pxs_cloud* c
 /* The data-parallel split of pxs_trainer_step_batch, for one trainer per GPU
  * over a shared cloud. pxs_trainer_accumulate renders and differentiates this
  * rank's `n_views` views (a graph replay when `graph` is nonzero) and leaves
- * the summed gradients in the trainer's device buffers with no optimiser
- * step; `loss` gets the mean loss of these views. The caller then sums the
- * buffers of pxs_trainer_gradients over the ranks (an all-reduce in place,
- * on or after the trainer's stream) and calls pxs_trainer_apply with the mean
- * loss over all ranks' views, which takes the Adam step and the schedule's
- * densify / opacity reset. Ranks that apply identical sums stay identical.
- * pxs_trainer_gradients returns device pointers: the gradient array
- * (values x count floats in the parameter layout), the screen gradient
- * (count floats) and the visible count (count int32), valid until the cloud
- * is resized (densify). */
+ * the step's sums in the trainer's reduction block with no optimiser step;
+ * `loss` (may be NULL) gets the mean loss of these views. The caller sums the
+ * block of pxs_trainer_reduction_block over the ranks (one all-reduce in
+ * place, on or after the trainer's stream) and calls pxs_trainer_apply, which
+ * takes the Adam step and the schedule's densify / opacity reset. With `loss`
+ * NaN, apply takes the mean loss over all ranks' views from the summed block,
+ * so no separate reduction of the loss is needed. Ranks that apply identical
+ * sums stay identical.
+ * The block is (values + 2) x count + 2 floats: the parameter gradients
+ * (values x count, the parameter layout), the screen gradient (count), the
+ * visible counts as floats (count; exact integers) and the loss tail (the
+ * rank's mean loss times its views, its views). pxs_trainer_gradients returns
+ * pointers to its first three parts. Both are device pointers, valid until the
+ * cloud is resized (densify). No reference counterpart: the reference trains
+ * on one device (SplatTrainer.cpp:326-362); its gradients are sums over views
+ * (SplatRaster.h:133-137), which is what makes the split exact. */
 int pxs_trainer_accumulate(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                            int32_t graph, float* loss);
 int pxs_trainer_apply(pxs_trainer* trainer, float loss);
+int pxs_trainer_reduction_block(pxs_trainer* trainer, float** block, int64_t* values);
 int pxs_trainer_gradients(pxs_trainer* trainer, float** params, float** screen_gradient,
-                          int32_t** visible_count, int32_t* count, int32_t* values);
+                          float** visible_count, int32_t* count, int32_t* values);
 
 /* Plain form of the same multi-view step: per-view kernel sequences with
  * host-synchronised sizes and no graph. Same arithmetic, same result. */
@@ -480,6 +487,21 @@ int pxs_downscale_to_width(pxs_context* context, const uint8_t* rgb, int32_t wid
 int pxs_trainer_ingest_images(pxs_trainer* trainer, int32_t n, const int32_t* view_ids,
                               const uint8_t* const* frames, const int32_t* widths,
                               const int32_t* heights);
+
+/* The same ingest, asynchronous, for a training loop that feeds each step's
+ * frames from host memory: the frames are copied to the device on the
+ * trainer's own copy stream while the current step runs, into one of two
+ * staging buffers, and are downscaled and converted into the views' training
+ * images (as pxs_trainer_ingest_images does) at the start of the next call
+ * that steps or replaces images (pxs_trainer_step, _step_batch, _step_views,
+ * _accumulate, _ingest_images, _set_images, or another stage call, which
+ * applies the earlier set first). The frames must stay valid and unchanged
+ * until that call returns; page-locked frames let the copy overlap the step.
+ * No reference counterpart: the reference converts on the host before
+ * training (Pipeline.cpp:1892-1917). */
+int pxs_trainer_stage_images(pxs_trainer* trainer, int32_t n, const int32_t* view_ids,
+                             const uint8_t* const* frames, const int32_t* widths,
+                             const int32_t* heights);
 
 /* ------------------------------------------------------- trained-cloud files
  * The reference's writers (GaussianCloud.h:95-131) into memory: the bytes of

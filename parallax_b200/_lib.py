@@ -78,9 +78,11 @@ def _declare(lib: ct.CDLL) -> None:
         "pxs_downscale_to_width": (ct.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
         "pxs_initialize_from_points": (ct.c_int, [_vp, _vp, _vp, _i32, _i32, _f32, _vp, _vp]),
         "pxs_trainer_ingest_images": (ct.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
+        "pxs_trainer_stage_images": (ct.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
         "pxs_trainer_export": (ct.c_int, [_vp, _i32, _i32, _vp, ct.c_size_t, _vp]),
         "pxs_trainer_apply": (ct.c_int, [_vp, _f32]),
         "pxs_trainer_gradients": (ct.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+        "pxs_trainer_reduction_block": (ct.c_int, [_vp, _vp, _vp]),
         "pxs_synthetic_cloud": (ct.c_int, [ct.c_uint64, _i32, _i32, _f32, _vp]),
         "pxs_synthetic_cameras": (ct.c_int, [ct.c_uint64, _i32, _i32, ct.c_double, _i32, _i32,
                                              ct.c_double, _vp]),

@@ -58,14 +58,43 @@ struct pxs_trainer {
   std::string error;
 
   int N = 0, S = 0, P = 14, cloud_sh = 0;
-  DeviceArray<float> params, grads, m, v, screen_gradient, acc_gradient;
+  DeviceArray<float> params, m, v, acc_gradient;
   DeviceArray<int32_t> visible_count, acc_views;
+  // The step's sums in one allocation, so a data-parallel caller sums them
+  // over the ranks with one collective: the parameter gradients (P x N), the
+  // screen gradient (N), the visible counts as floats (N, exact integers; the
+  // kernels count in visible_count and accumulate() copies them here) and a
+  // loss tail (the mean loss of this rank's views times their number, and the
+  // number), from which apply() takes the mean over all ranks' views.
+  DeviceArray<float> grad_block;
+  size_t n_alloc() const { return static_cast<size_t>(std::max(N, 1)); }
+  float* d_grads() const { return grad_block.get(); }
+  float* d_screen() const { return grad_block.get() + static_cast<size_t>(P) * n_alloc(); }
+  float* d_visible_f() const { return d_screen() + n_alloc(); }
+  float* d_loss_tail() const { return d_visible_f() + n_alloc(); }
+  size_t block_values() const { return static_cast<size_t>(P + 2) * n_alloc() + 2; }
   DeviceArray<float> next_params, next_m, next_v;
 
   std::vector<pxs_camera> cameras;
   std::vector<int64_t> image_offset;  // first pixel of each view in `images`
   DeviceArray<float> images;
   DeviceArray<uint8_t> ingest_in;  // staging for 8-bit frames
+
+  // Frames staged for a coming step (pxs_trainer_stage_images): copied to
+  // the device on copy_stream, into one of two staging buffers, while the
+  // current step runs, then converted into the image store on `stream` before
+  // the next step's kernels. A staging buffer is refilled only after the
+  // conversion that read it (consumed_event) has run.
+  struct StagedFrame {
+    int view, width, height, out_width, out_height;
+    size_t offset;
+  };
+  cudaStream_t copy_stream = nullptr;
+  DeviceArray<uint8_t> stage_buf[2];
+  cudaEvent_t staged_event[2] = {}, consumed_event[2] = {};
+  bool consumed_recorded[2] = {false, false};
+  std::vector<StagedFrame> pending;
+  int pending_slot = -1, next_slot = 0;
 
   int iteration = 0;
   float extent = 1.f, last_loss = 0.f, smoothed_loss = 0.f;
@@ -105,8 +134,14 @@ struct pxs_trainer {
   DeviceArray<unsigned long long> pair_counts;
 
   ~pxs_trainer() {
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     graph.reset();
     graph_acc.reset();
+    for (int k = 0; k < 2; ++k) {
+      if (staged_event[k]) cudaEventDestroy(staged_event[k]);
+      if (consumed_event[k]) cudaEventDestroy(consumed_event[k]);
+    }
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (cudaEvent_t& e : events)
       if (e) cudaEventDestroy(e);
     if (host_loss) cudaFreeHost(host_loss);
@@ -197,8 +232,8 @@ struct pxs_trainer {
   }
 
   void adam() {
-    pxs::launch_adam(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(), 1,
-                     screen_gradient.get(), visible_count.get(), acc_gradient.get(),
+    pxs::launch_adam(params.get(), d_grads(), m.get(), v.get(), N, S, scalars.get(), 1,
+                     d_screen(), visible_count.get(), acc_gradient.get(),
                      acc_views.get(), stream, position_scales());
     PXS_CUDA(cudaGetLastError());
   }
@@ -258,16 +293,84 @@ struct pxs_trainer {
   void resize_state() {
     ++generation;
     const size_t n = static_cast<size_t>(std::max(N, 1));
-    grads.reserve(static_cast<size_t>(P) * n);
-    screen_gradient.reserve(n);
+    grad_block.reserve(block_values());
     visible_count.reserve(n);
     acc_gradient.reserve(n);
     acc_views.reserve(n);
-    PXS_CUDA(cudaMemsetAsync(grads.get(), 0, sizeof(float) * P * n, stream));
-    PXS_CUDA(cudaMemsetAsync(screen_gradient.get(), 0, sizeof(float) * n, stream));
+    PXS_CUDA(cudaMemsetAsync(grad_block.get(), 0, sizeof(float) * block_values(), stream));
     PXS_CUDA(cudaMemsetAsync(visible_count.get(), 0, sizeof(int32_t) * n, stream));
     PXS_CUDA(cudaMemsetAsync(acc_gradient.get(), 0, sizeof(float) * n, stream));
     PXS_CUDA(cudaMemsetAsync(acc_views.get(), 0, sizeof(int32_t) * n, stream));
+  }
+
+  // ---------------------------------------------------------- staged ingest
+
+  // Enqueues, on `stream`, the conversion of the staged frames into the
+  // image store, after their copy; the staging buffer is then free to refill.
+  void consume_staged() {
+    if (pending_slot < 0) return;
+    const int k = pending_slot;
+    PXS_CUDA(cudaStreamWaitEvent(stream, staged_event[k], 0));
+    for (const StagedFrame& f : pending) {
+      pxs::launch_downscale(stage_buf[k].get() + f.offset, f.width, f.height, f.out_width,
+                            f.out_height, nullptr,
+                            images.get() + image_offset[static_cast<size_t>(f.view)] * 3, stream);
+      PXS_CUDA(cudaGetLastError());
+    }
+    PXS_CUDA(cudaEventRecord(consumed_event[k], stream));
+    consumed_recorded[k] = true;
+    pending.clear();
+    pending_slot = -1;
+  }
+
+  void stage_frames(int n, const int32_t* ids, const uint8_t* const* frames,
+                    const int32_t* widths, const int32_t* heights) {
+    std::vector<StagedFrame> staged;
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+      const int id = ids[i];
+      if (id < 0 || id >= static_cast<int>(cameras.size()))
+        throw Error(PXS_ERR_INVALID, "view id out of range");
+      const pxs_camera& cam = cameras[static_cast<size_t>(id)];
+      int w = 0, h = 0;
+      pxs::downscaled_size(widths[i], heights[i], cam.width, &w, &h);
+      if (w != cam.width || h != cam.height)
+        throw Error(PXS_ERR_INVALID, "the downscaled frame does not match the view's size");
+      const size_t bytes = static_cast<size_t>(widths[i]) * heights[i] * 3;
+      if (bytes == 0) continue;
+      if (frames[i] == nullptr) throw Error(PXS_ERR_INVALID, "frame is null");
+      staged.push_back({id, widths[i], heights[i], w, h, total});
+      total += (bytes + 255) / 256 * 256;
+    }
+    // frames staged earlier take effect first
+    consume_staged();
+    if (staged.empty()) return;
+    if (copy_stream == nullptr) {
+      PXS_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+      for (int k = 0; k < 2; ++k) {
+        PXS_CUDA(cudaEventCreateWithFlags(&staged_event[k], cudaEventDisableTiming));
+        PXS_CUDA(cudaEventCreateWithFlags(&consumed_event[k], cudaEventDisableTiming));
+      }
+    }
+    const int k = next_slot;
+    next_slot ^= 1;
+    if (total > stage_buf[k].capacity()) {
+      // grown only when both streams are idle
+      PXS_CUDA(cudaStreamSynchronize(stream));
+      PXS_CUDA(cudaStreamSynchronize(copy_stream));
+      stage_buf[k].reserve(total);
+    }
+    if (consumed_recorded[k]) PXS_CUDA(cudaStreamWaitEvent(copy_stream, consumed_event[k], 0));
+    for (size_t i = 0, j = 0; i < static_cast<size_t>(n); ++i) {
+      const size_t bytes = static_cast<size_t>(widths[i]) * heights[i] * 3;
+      if (bytes == 0) continue;
+      const StagedFrame& f = staged[j++];
+      PXS_CUDA(cudaMemcpyAsync(stage_buf[k].get() + f.offset, frames[i], bytes,
+                               cudaMemcpyHostToDevice, copy_stream));
+    }
+    PXS_CUDA(cudaEventRecord(staged_event[k], copy_stream));
+    pending = std::move(staged);
+    pending_slot = k;
   }
 
   // ---------------------------------------------------------- steps
@@ -284,6 +387,7 @@ struct pxs_trainer {
   // SplatTrainer::step (SplatTrainer.cpp:326-362): one view, synchronised.
   bool step() {
     if (schedule_done()) return false;
+    consume_staged();
     const int id = next_view();
     const pxs::ViewBatch b = batch_for({id});
     frame.prepare(b, N, S, stream);
@@ -293,7 +397,7 @@ struct pxs_trainer {
     float* d_dL = dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
     frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
     frame.backward(d_dL, stream);
-    frame.param_grads(params.get(), grads.get(), screen_gradient.get(), visible_count.get(),
+    frame.param_grads(params.get(), d_grads(), d_screen(), visible_count.get(),
                       stream);
     PXS_CUDA(cudaMemcpyAsync(host_loss, frame.loss_total.get(), sizeof(float),
                              cudaMemcpyDeviceToHost, stream));
@@ -306,6 +410,7 @@ struct pxs_trainer {
   }
 
   std::vector<int> take_views(int n_views, const int32_t* ids) {
+    consume_staged();
     std::vector<int> out;
     for (int i = 0; i < n_views; ++i) {
       const int id = ids != nullptr ? ids[i] : next_view();
@@ -333,7 +438,7 @@ struct pxs_trainer {
       float* d_dL = dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
       frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
       frame.backward(d_dL, stream);
-      frame.param_grads(params.get(), grads.get(), screen_gradient.get(), visible_count.get(),
+      frame.param_grads(params.get(), d_grads(), d_screen(), visible_count.get(),
                         stream);
       PXS_CUDA(cudaMemcpyAsync(acc + i, frame.loss_total.get(), sizeof(float),
                                cudaMemcpyDeviceToDevice, stream));
@@ -389,12 +494,15 @@ struct pxs_trainer {
     mark(4);
     frame.backward(dL.get(), stream);
     mark(5);
-    frame.param_grads(params.get(), grads.get(), screen_gradient.get(), visible_count.get(),
+    frame.param_grads(params.get(), d_grads(), d_screen(), visible_count.get(),
                       stream);
     mark(6);
+    if (!with_adam)
+      pxs::launch_pack_reduction(visible_count.get(), d_visible_f(), N, frame.loss_total.get(),
+                                 frame.V, d_loss_tail(), stream);
     if (with_adam)
-      pxs::launch_adam_checked(params.get(), grads.get(), m.get(), v.get(), N, S, scalars.get(),
-                               screen_gradient.get(), visible_count.get(), acc_gradient.get(),
+      pxs::launch_adam_checked(params.get(), d_grads(), m.get(), v.get(), N, S, scalars.get(),
+                               d_screen(), visible_count.get(), acc_gradient.get(),
                                acc_views.get(), frame.overflow.get(), stream,
                                position_scales());
     mark(7);
@@ -470,8 +578,7 @@ struct pxs_trainer {
         return;
       }
       // the pairs did not fit: nothing of this step counts; grow and redo
-      PXS_CUDA(cudaMemsetAsync(grads.get(), 0, sizeof(float) * P * std::max(N, 1), stream));
-      PXS_CUDA(cudaMemsetAsync(screen_gradient.get(), 0, sizeof(float) * std::max(N, 1), stream));
+      PXS_CUDA(cudaMemsetAsync(d_grads(), 0, sizeof(float) * (P + 1) * n_alloc(), stream));
       PXS_CUDA(cudaMemsetAsync(visible_count.get(), 0, sizeof(int32_t) * std::max(N, 1), stream));
       frame.project(params.get(), stream);
       const int64_t K = frame.bin(true, stream);
@@ -577,6 +684,16 @@ struct pxs_trainer {
 
   void apply(float loss) {
     if (!pending_apply) throw Error(PXS_ERR_INVALID, "apply without accumulate");
+    if (std::isnan(loss)) {
+      // the mean over every rank's views, from the summed loss tail
+      float tail[2];
+      PXS_CUDA(cudaMemcpyAsync(tail, d_loss_tail(), sizeof(tail), cudaMemcpyDeviceToHost,
+                               stream));
+      PXS_CUDA(cudaStreamSynchronize(stream));
+      loss = tail[1] > 0.f ? tail[0] / tail[1] : 0.f;
+    }
+    // the (summed) visible counts back to the integers the statistics keep
+    pxs::launch_unpack_visible(d_visible_f(), visible_count.get(), N, stream);
     upload_scalars();
     adam();
     PXS_CUDA(cudaStreamSynchronize(stream));
@@ -757,13 +874,20 @@ int pxs_trainer_apply(pxs_trainer* t, float loss) {
 }
 
 int pxs_trainer_gradients(pxs_trainer* t, float** params, float** screen_gradient,
-                          int32_t** visible_count, int32_t* count, int32_t* values) {
+                          float** visible_count, int32_t* count, int32_t* values) {
   return guarded(t, [&] {
-    if (params) *params = t->grads.get();
-    if (screen_gradient) *screen_gradient = t->screen_gradient.get();
-    if (visible_count) *visible_count = t->visible_count.get();
+    if (params) *params = t->d_grads();
+    if (screen_gradient) *screen_gradient = t->d_screen();
+    if (visible_count) *visible_count = t->d_visible_f();
     if (count) *count = t->N;
     if (values) *values = t->P;
+  });
+}
+
+int pxs_trainer_reduction_block(pxs_trainer* t, float** block, int64_t* values) {
+  return guarded(t, [&] {
+    if (block) *block = t->grad_block.get();
+    if (values) *values = static_cast<int64_t>(t->block_values());
   });
 }
 
@@ -868,6 +992,7 @@ int pxs_trainer_pair_stats(pxs_trainer* t, int64_t* evaluated, int64_t* contribu
 int pxs_trainer_set_images(pxs_trainer* t, int32_t n, const int32_t* view_ids,
                            const float* const* images) {
   return guarded(t, [&] {
+    t->consume_staged();
     for (int i = 0; i < n; ++i) {
       const int id = view_ids[i];
       if (id < 0 || id >= static_cast<int>(t->cameras.size()))
@@ -933,6 +1058,17 @@ int pxs_trainer_finish(pxs_trainer* t, float* params, int32_t capacity, int32_t*
   });
 }
 
+int pxs_trainer_stage_images(pxs_trainer* t, int32_t n, const int32_t* view_ids,
+                             const uint8_t* const* frames, const int32_t* widths,
+                             const int32_t* heights) {
+  return guarded(t, [&] {
+    if (n < 0 || (n > 0 && (view_ids == nullptr || frames == nullptr || widths == nullptr ||
+                            heights == nullptr)))
+      throw Error(PXS_ERR_INVALID, "null argument");
+    t->stage_frames(n, view_ids, frames, widths, heights);
+  });
+}
+
 int pxs_trainer_ingest_images(pxs_trainer* t, int32_t n, const int32_t* view_ids,
                               const uint8_t* const* frames, const int32_t* widths,
                               const int32_t* heights) {
@@ -940,6 +1076,7 @@ int pxs_trainer_ingest_images(pxs_trainer* t, int32_t n, const int32_t* view_ids
     if (n < 0 || (n > 0 && (view_ids == nullptr || frames == nullptr || widths == nullptr ||
                             heights == nullptr)))
       throw Error(PXS_ERR_INVALID, "null argument");
+    t->consume_staged();
     for (int i = 0; i < n; ++i) {
       const int id = view_ids[i];
       if (id < 0 || id >= static_cast<int>(t->cameras.size()))

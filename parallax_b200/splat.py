@@ -385,19 +385,29 @@ class SplatTrainer:
                                                      ct.byref(loss)))
         return loss.value
 
-    def apply(self, loss: float) -> None:
-        """The second half: the Adam step with the (summed) gradient buffers."""
+    def apply(self, loss: float = float("nan")) -> None:
+        """The second half: the Adam step with the (summed) reduction block. With
+        `loss` NaN the mean loss over all ranks' views comes from the block."""
         self._check(self._lib.pxs_trainer_apply(self.handle, ct.c_float(loss)))
 
+    def reduction_block(self):
+        """(device pointer, float count) of the one buffer a data-parallel step
+        sums over the ranks: gradients, screen gradient, visible counts and the
+        loss tail (pxs_trainer_reduction_block)."""
+        b, n = ct.c_void_p(), ct.c_int64()
+        self._check(self._lib.pxs_trainer_reduction_block(self.handle, ct.byref(b), ct.byref(n)))
+        return b.value, n.value
+
     def gradient_buffers(self):
-        """Device pointers of the gradient buffers that a data-parallel step sums
-        over ranks: [(pointer, element count, 'float32' | 'int32'), ...]."""
+        """Device pointers of the gradient parts of the reduction block:
+        [(pointer, element count, 'float32'), ...] for the parameter gradients,
+        the screen gradient and the visible counts (as floats)."""
         g, sg, vc = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
         n, P = ct.c_int32(), ct.c_int32()
         self._check(self._lib.pxs_trainer_gradients(self.handle, ct.byref(g), ct.byref(sg),
                                                     ct.byref(vc), ct.byref(n), ct.byref(P)))
         return [(g.value, P.value * n.value, "float32"), (sg.value, n.value, "float32"),
-                (vc.value, n.value, "int32")]
+                (vc.value, n.value, "float32")]
 
     def ingest_images(self, view_ids: Sequence[int], frames: Sequence[np.ndarray],
                       sizes: Sequence[Tuple[int, int]]) -> None:
@@ -410,6 +420,23 @@ class SplatTrainer:
         ws = (ct.c_int32 * max(n, 1))(*[s[0] for s in sizes])
         hs = (ct.c_int32 * max(n, 1))(*[s[1] for s in sizes])
         self._check(self._lib.pxs_trainer_ingest_images(self.handle, n, ids, ptrs, ws, hs))
+
+    def stage_images(self, view_ids: Sequence[int], frames: Sequence[np.ndarray],
+                     sizes: Sequence[Tuple[int, int]]) -> None:
+        """ingest_images without waiting: the frames are copied to the device
+        while the current step runs and take effect at the next step (or the
+        next ingest / set_images / stage call). The frames are kept referenced
+        here until then; they must not be modified before that call returns."""
+        n = len(view_ids)
+        keep = [f if isinstance(f, np.ndarray) and f.dtype == np.uint8 and f.flags.c_contiguous
+                else np.ascontiguousarray(f, dtype=np.uint8) for f in frames]
+        ids = (ct.c_int32 * max(n, 1))(*view_ids)
+        ptrs = (ct.c_void_p * max(n, 1))(*[f.ctypes.data for f in keep])
+        ws = (ct.c_int32 * max(n, 1))(*[s[0] for s in sizes])
+        hs = (ct.c_int32 * max(n, 1))(*[s[1] for s in sizes])
+        self._check(self._lib.pxs_trainer_stage_images(self.handle, n, ids, ptrs, ws, hs))
+        # held until a later stage call: the copy may still be reading them
+        self._staged = getattr(self, "_staged", [])[-1:] + [keep]
 
     def export(self, fmt: str = "ply", fractional_bits: int = 12) -> bytes:
         """The trained cloud as the bytes of a .ply, .splat or .spz file."""

@@ -90,3 +90,38 @@ def test_seed_matches_the_reference(n, sh, with_colors):
     ref = reference_seed(points, colors, sh, 0.1)
     assert ours.params.shape == ref.shape
     assert np.array_equal(ours.params.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_staged_frames_train_like_ingested_frames():
+    """pxs_trainer_stage_images, pipelined the way a feeding loop uses it (the
+    next step's frames staged before the current step runs), takes the same
+    steps as ingesting each step's frames synchronously: same losses and the
+    same cloud, bit for bit."""
+    params, rest = O.random_cloud(72, 3000, 1)
+    cloud = px.GaussianCloud(params, 1, rest)
+    views = O.orbit_views(6, 160, 120, seed=4)
+    blank = np.zeros(160 * 120 * 3, np.float32)
+    rs = np.random.default_rng(9)
+    frames = [rs.integers(0, 256, 640 * 480 * 3, dtype=np.uint8) for _ in range(6)]
+    schedule = [[0, 1], [2, 3], [4, 5], [1, 4], [3, 0]]
+    cfg = px.TrainConfig(iterations=50, sh_degree=1, sh_increase_interval=0)
+    sync = px.SplatTrainer(cloud, [(v.camera(), blank) for v in views], cfg)
+    staged = px.SplatTrainer(cloud, [(v.camera(), blank) for v in views], cfg)
+    losses_sync, losses_staged = [], []
+    for ids in schedule:
+        sync.ingest_images(ids, [frames[i] for i in ids], [(640, 480)] * len(ids))
+        losses_sync.append(sync.step_batch(len(ids), ids))
+    staged.stage_images(schedule[0], [frames[i] for i in schedule[0]], [(640, 480)] * 2)
+    for s, ids in enumerate(schedule):
+        if s + 1 < len(schedule):
+            nxt = schedule[s + 1]
+            staged.stage_images(nxt, [frames[i] for i in nxt], [(640, 480)] * len(nxt))
+        losses_staged.append(staged.step_batch(len(ids), ids))
+    assert losses_sync == losses_staged
+    assert np.array_equal(sync.cloud_params().view(np.uint32),
+                          staged.cloud_params().view(np.uint32))
+    with pytest.raises(px.PxsError):  # the wrong frame size is refused before any copy
+        staged.stage_images([0], [np.zeros(640 * 400 * 3, np.uint8)], [(640, 400)])
+    for t in (sync, staged):
+        t.close()
