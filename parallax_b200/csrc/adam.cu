@@ -150,3 +150,41 @@ void launch_reset_opacity(float* params, float* m, float* v, int N, float ceilin
 }
 
 }  // namespace pxs
+
+namespace pxs {
+
+// The data-parallel reduction block's small parts (see pxs_trainer_accumulate):
+// the visible counts as floats (exact for counts below 2^24) and the loss tail
+// (mean loss x views, views), so one collective sums everything.
+__global__ void k_pack_reduction(const int32_t* __restrict__ visible, float* __restrict__ visible_f,
+                                 int N, const float* __restrict__ loss_mean, int n_views,
+                                 float* __restrict__ tail) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < N) visible_f[g] = (float)visible[g];
+  if (g == 0) {
+    tail[0] = loss_mean[0] * (float)n_views;
+    tail[1] = (float)n_views;
+  }
+}
+
+__global__ void k_unpack_visible(const float* __restrict__ visible_f,
+                                 int32_t* __restrict__ visible, int N) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < N) visible[g] = (int32_t)rintf(visible_f[g]);
+}
+
+void launch_pack_reduction(const int32_t* visible, float* visible_f, int N,
+                           const float* loss_mean, int n_views, float* tail,
+                           cudaStream_t stream) {
+  count_launch();
+  k_pack_reduction<<<(std::max(N, 1) + 255) / 256, 256, 0, stream>>>(visible, visible_f, N,
+                                                                     loss_mean, n_views, tail);
+}
+
+void launch_unpack_visible(const float* visible_f, int32_t* visible, int N, cudaStream_t stream) {
+  if (N <= 0) return;
+  count_launch();
+  k_unpack_visible<<<(N + 255) / 256, 256, 0, stream>>>(visible_f, visible, N);
+}
+
+}  // namespace pxs

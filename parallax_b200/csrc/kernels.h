@@ -159,6 +159,10 @@ float measure_fp32_peak_tflops(cudaStream_t stream);
 // adam.cu
 // `position_scale` (N floats, optional) multiplies the position learning rate
 // per gaussian: each scene's extent, when one cloud holds several scenes.
+void launch_pack_reduction(const int32_t* visible, float* visible_f, int N,
+                           const float* loss_mean, int n_views, float* tail,
+                           cudaStream_t stream);
+void launch_unpack_visible(const float* visible_f, int32_t* visible, int N, cudaStream_t stream);
 void launch_adam(float* params, float* grads, float* m, float* v, int N, int S,
                  const StepScalars* scalars, int zero_grads, float* screen_gradient,
                  int32_t* visible_count, float* acc_gradient, int32_t* acc_views,

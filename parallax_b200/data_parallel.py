@@ -3,10 +3,12 @@
 The reference trains one view per step on one device (SplatTrainer.cpp:326-362).
 Its gradients are sums over views (SplatRaster.h:133-137), so a step over the
 views of several GPUs is: every rank renders and differentiates its own views
-(pxs_trainer_accumulate), the gradient buffers are summed over the ranks in
-place (one all-reduce per buffer), and every rank takes the same Adam step with
-the same sums (pxs_trainer_apply). The densify decisions depend only on those
-sums and on the cloud, so the replicas stay identical.
+(pxs_trainer_accumulate), the trainer's reduction block -- parameter
+gradients, screen gradient, visible counts and the loss -- is summed over the
+ranks with one all-reduce in place, and every rank takes the same Adam step
+with the same sums (pxs_trainer_apply), reading the mean loss over all ranks'
+views from the block. The densify decisions depend only on those sums and on
+the cloud, so the replicas stay identical.
 """
 from __future__ import annotations
 
@@ -40,48 +42,47 @@ def all_reduce_sum(tensors, group=None) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
 
 
-def mean_loss(loss: float, n_views: int, group=None, device: str = "cpu") -> float:
-    """The mean loss over every rank's views, from this rank's mean."""
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([loss * n_views, float(n_views)], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-    return float(t[0] / t[1]) if t[1] > 0 else 0.0
+def _block_tensor(block):
+    """A trainer's reduction block as a tensor: a (device pointer, float count)
+    pair is aliased in place; a tensor is taken as it is."""
+    if isinstance(block, tuple):
+        return device_tensors([(block[0], block[1], "float32")])[0]
+    return block
 
 
 class DataParallelStep:
     """One data-parallel step of `trainer` (a SplatTrainer, or anything with
-    accumulate / apply / gradient tensors):
+    accumulate / apply / reduction_block):
 
         step = DataParallelStep(trainer)
-        loss = step(view_ids_of_this_rank)
+        step(view_ids_of_this_rank)
 
-    `buffers` returns the tensors to sum (default: the trainer's device
-    gradient buffers); `reduce` sums them over the ranks (default: an
-    all-reduce over `group`); `device` is where the loss is reduced."""
+    `block` returns the one tensor to sum (default: the trainer's device
+    reduction block); `reduce` sums a list of tensors over the ranks (default:
+    an all-reduce over `group`); `device` "cuda" runs the sum on the trainer's
+    stream. Returns the trainer's last loss when it has one."""
 
-    def __init__(self, trainer, group=None, buffers: Optional[Callable[[], list]] = None,
+    def __init__(self, trainer, group=None, block: Optional[Callable[[], object]] = None,
                  reduce: Optional[Callable[[list], None]] = None, device: str = "cuda",
                  graph: bool = True):
         self.trainer = trainer
         self.group = group
-        self.buffers = buffers or (lambda: device_tensors(trainer.gradient_buffers()))
+        self.block = block or (lambda: _block_tensor(trainer.reduction_block()))
         self.reduce = reduce or (lambda ts: all_reduce_sum(ts, group))
         self.device = device
         self.graph = graph
 
-    def __call__(self, view_ids: Sequence[int]) -> float:
-        loss = self.trainer.accumulate(view_ids, self.graph)
+    def __call__(self, view_ids: Sequence[int]):
+        self.trainer.accumulate(view_ids, self.graph)
         if self.device == "cuda":
-            # the sums run ordered on the trainer's stream, so its Adam step
-            # (queued by apply) waits for them
+            # the sum runs ordered on the trainer's stream, so the Adam step
+            # that apply queues there waits for it
             import torch
 
             with torch.cuda.stream(torch.cuda.ExternalStream(self.trainer.stream())):
-                self.reduce(self.buffers())
+                self.reduce([self.block()])
         else:
-            self.reduce(self.buffers())
-        total = mean_loss(loss, len(view_ids), self.group, self.device)
-        self.trainer.apply(total)
-        return total
+            self.reduce([self.block()])
+        self.trainer.apply(float("nan"))  # the mean loss comes from the summed block
+        last = getattr(self.trainer, "last_loss", None)
+        return last() if callable(last) else last
