@@ -27,6 +27,7 @@
 
 #ifdef PXREF_SHIM
 #include <algorithm>
+#include <chrono>
 #include <limits>
 #include <stdexcept>
 
@@ -620,6 +621,32 @@ int ref_write_cloud(const float* params, int n, int rest, int cloud_sh, int form
 
 // downscaleToWidth (ImageIo.cpp:300-337); returns the output width and height
 // through w / h and writes the bytes when `out` is given.
+// readGaussianPly and GaussianCloud::isValid (GaussianCloud.cpp) on a file:
+// the count, whether it is valid, and the least opacity. Returns 1 when read.
+int ref_read_ply_stats(const char* path, int* count, int* valid, float* min_opacity,
+                       char* reason, int reason_len) {
+  GaussianCloud cloud;
+  std::string error;
+  if (!readGaussianPly(path, &cloud, &error)) {
+    if (reason != nullptr && reason_len > 0) {
+      std::strncpy(reason, error.c_str(), static_cast<size_t>(reason_len) - 1);
+      reason[reason_len - 1] = '\0';
+    }
+    return 0;
+  }
+  *count = static_cast<int>(cloud.size());
+  std::string why;
+  *valid = cloud.isValid(&why) ? 1 : 0;
+  float least = 1.f;
+  for (const Gaussian& g : cloud.gaussians) least = std::min(least, gaussianOpacity(g));
+  *min_opacity = least;
+  if (reason != nullptr && reason_len > 0) {
+    std::strncpy(reason, why.c_str(), static_cast<size_t>(reason_len) - 1);
+    reason[reason_len - 1] = '\0';
+  }
+  return 1;
+}
+
 void ref_downscale(const uint8_t* rgb, int width, int height, int target_width, uint8_t* out,
                    int* w, int* h) {
   ColorBuffer image(width, height);
@@ -798,6 +825,152 @@ int ref_shim_train_splats_on_gpu(float* params, int n, int rest, int cloud_sh, i
   *count = fromCloud(cloud, rest, params, std::max(n, config->max_gaussians));
   *sh_degree = cloud.sh_degree;
   return 1;
+}
+
+// The splat stage of the reference pipeline (Pipeline::Impl::runSplatTraining,
+// Pipeline.cpp:1844-2009) from the coloured point cloud and the posed frames
+// on, as a test driver: the seed budget and point stride (:1858-1874), the
+// seed by initializeFromPointCloud, the training views spread over the frames
+// and downscaled by downscaleToWidth then divided by 255 (:1888-1917), the
+// training config derived from the stage's settings (:1922-1929), the
+// progress callback with the cancel token and the time budget (:1931-1957),
+// trainSplatsOnGpu -- here the CUDA shim -- with the CPU trainer as the
+// fallback (:1959-1991), and the outcome note (:1993-2009). The pipeline's
+// checkpoint files and the rest of its stages are not part of it; the caller
+// writes the field with the reference's writer and reads it back.
+// settings: iterations, max_gaussians, sh_degree, image_width, max_views,
+// time_budget_ms (0: none), cancel_at (the iteration at which the cancel token
+// is set; 0: never). Frames are 8-bit RGB at sizes[2f], sizes[2f+1] with
+// intrinsics K[4f..] for that size. Returns 1 for a successful outcome.
+int ref_shim_pipeline_splat_stage(const float* points, const uint8_t* colors, int n_points,
+                                  int n_frames, const double* K, const int32_t* sizes,
+                                  const double* R, const double* t,
+                                  const uint8_t* const* frames, const int32_t* settings,
+                                  float* params_out, int capacity, int32_t* out_count,
+                                  int32_t* out_rest, int32_t* out_sh, int32_t* cancelled,
+                                  char* backend, int backend_len, char* message,
+                                  int message_len) {
+  const int iterations = settings[0], max_gaussians = settings[1], sh = settings[2];
+  const int image_width = settings[3], max_views = settings[4];
+  const long long budget_ms = settings[5];
+  const int cancel_at = settings[6];
+  bool token = false;  // the cancel token
+  std::string used;
+  auto outcome = [&](bool success, bool was_cancelled, const std::string& note) {
+    *cancelled = was_cancelled ? 1 : 0;
+    if (message != nullptr && message_len > 0) {
+      std::strncpy(message, note.c_str(), static_cast<size_t>(message_len) - 1);
+      message[message_len - 1] = '\0';
+    }
+    if (backend != nullptr && backend_len > 0) {
+      std::strncpy(backend, used.c_str(), static_cast<size_t>(backend_len) - 1);
+      backend[backend_len - 1] = '\0';
+    }
+    return success ? 1 : 0;
+  };
+
+  // seed from at most a quarter of the budget: every k-th point
+  std::vector<Vec3f> pts;
+  std::vector<std::array<uint8_t, 3>> cols;
+  const size_t n = static_cast<size_t>(std::max(n_points, 0));
+  const size_t seed_budget = std::max<size_t>(1, static_cast<size_t>(max_gaussians) / 4);
+  const size_t stride = n > seed_budget ? (n + seed_budget - 1) / seed_budget : 1;
+  for (size_t i = 0; i < n; i += stride) {
+    pts.emplace_back(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    cols.push_back({colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]});
+  }
+  if (pts.empty()) return outcome(true, false, "no point cloud to seed the splat field from");
+  GaussianCloud cloud = initializeFromPointCloud(pts, cols, sh);
+  if (cloud.empty()) return outcome(false, false, "the point cloud produced no gaussians");
+
+  // training views spread evenly over the frames
+  const size_t view_budget = std::min<size_t>(static_cast<size_t>(n_frames),
+                                              static_cast<size_t>(std::max(4, max_views)));
+  std::vector<SplatTrainingView> views;
+  for (size_t v = 0; v < view_budget; ++v) {
+    const size_t f = view_budget == 1
+                         ? 0
+                         : static_cast<size_t>(static_cast<double>(v) * (n_frames - 1) /
+                                               (view_budget - 1));
+    ColorBuffer image;
+    image.width = sizes[2 * f];
+    image.height = sizes[2 * f + 1];
+    image.pixels.assign(frames[f],
+                        frames[f] + static_cast<size_t>(image.width) * image.height * 3);
+    const ColorBuffer scaled = downscaleToWidth(image, image_width);
+    SplatTrainingView tv;
+    tv.view = toView(K + 4 * f, image.width, image.height, R + 9 * f, t + 3 * f);
+    tv.view.intrinsics = tv.view.intrinsics.scaledTo(scaled.width, scaled.height);
+    tv.image.resize(static_cast<size_t>(scaled.width) * scaled.height * 3);
+    for (size_t p = 0; p < tv.image.size(); ++p)
+      tv.image[p] = static_cast<float>(scaled.pixels[p]) / 255.f;
+    views.push_back(std::move(tv));
+  }
+  if (views.size() < 2)
+    return outcome(false, false, "at least two posed views are needed to train splats");
+
+  SplatTrainingConfig tc;
+  tc.iterations = std::max(1, iterations);
+  tc.sh_degree = sh;
+  tc.max_gaussians = max_gaussians;
+  tc.densify_until_iteration = tc.iterations / 2;
+  tc.opacity_reset_interval = std::max(1, tc.iterations / 3);
+  tc.sh_increase_interval = std::max(1, tc.iterations / 8);
+  const std::string invalid = tc.validate();
+  if (!invalid.empty()) return outcome(false, false, invalid);
+
+  bool was_cancelled = false, out_of_time = false;
+  int done = 0;
+  const auto started = std::chrono::steady_clock::now();
+  const SplatTrainingCallback callback = [&](const SplatTrainingProgress& p) {
+    if (cancel_at > 0 && p.iteration >= cancel_at) token = true;
+    if (token) {
+      was_cancelled = true;
+      return false;
+    }
+    done = p.iteration;
+    if (budget_ms > 0) {
+      const auto elapsed = std::chrono::duration_cast<std::chrono::milliseconds>(
+                               std::chrono::steady_clock::now() - started)
+                               .count();
+      if (elapsed >= budget_ms) {
+        out_of_time = true;
+        return false;
+      }
+    }
+    return true;
+  };
+
+  std::string gpu_error;
+  if (trainSplatsOnGpu(&cloud, views, tc, callback, &gpu_error)) {
+    used = "gpu";
+  } else if (was_cancelled) {
+    return outcome(false, true, "cancelled");
+  } else if (out_of_time) {
+    used = "gpu";
+  } else {
+    // no usable device: the reduced CPU run
+    SplatTrainingConfig reduced = tc;
+    reduced.iterations = std::max(1, tc.iterations / 5);
+    reduced.max_gaussians = std::min(tc.max_gaussians, 60000);
+    reduced.densify_until_iteration = reduced.iterations / 2;
+    reduced.opacity_reset_interval = std::max(1, reduced.iterations / 3);
+    reduced.sh_increase_interval = std::max(1, reduced.iterations / 8);
+    reduced.sh_degree = std::min(1, sh);
+    SplatTrainer trainer(std::move(cloud), std::move(views), reduced);
+    if (!trainer.train(callback) && was_cancelled) return outcome(false, true, "cancelled");
+    cloud = trainer.finish();
+    used = "cpu";
+  }
+  if (token) return outcome(false, true, "cancelled");
+  const int rest = cloud.gaussians.empty() ? 0 : static_cast<int>(cloud.gaussians[0].sh_rest.size()) / 3;
+  *out_rest = rest;
+  *out_sh = cloud.sh_degree;
+  *out_count = fromCloud(cloud, rest, params_out, capacity);
+  std::string note = std::to_string(cloud.size()) + " gaussians (" + used + ")";
+  if (out_of_time)
+    note += ", stopped at iteration " + std::to_string(done) + " when the time budget ran out";
+  return outcome(true, false, note);
 }
 #endif  // PXREF_SHIM
 

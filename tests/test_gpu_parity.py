@@ -37,6 +37,9 @@ import oracle_lib as O
 import parallax_b200 as px
 from parallax_b200._abi import PROJECTED_DTYPE, RasterOptions, TrainConfig
 
+# Loss drift allowed over the 60-step trainer run (relative, worst step).
+LOSS_DRIFT = 1e-3
+
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -476,7 +479,7 @@ def blob_scene(n_views=4, size=24):
 def test_trainer_follows_the_reference_schedule():
     """The golden trainer run (SplatTrainerTest.cpp blob scene, 60 iterations,
     densify every 20): same view order, same counts after each densify, losses
-    within 1e-2 relative, same finished count."""
+    within LOSS_DRIFT relative (the first step within 1e-5), same finished count."""
     d = load("trainer_blobs.npz")
     n_views = int(d["n_views"])
     views = []
@@ -493,7 +496,12 @@ def test_trainer_follows_the_reference_schedule():
         counts.append(st["count"])
     assert counts == list(d["counts"])
     rel = np.abs(np.array(losses) - d["losses"]) / np.abs(d["losses"])
-    assert rel.max() <= 1e-2, rel.max()
+    # the first step differs only by the device's summation order; later steps
+    # carry that difference forward through Adam and two densify steps
+    print("loss drift against the reference run: first step %.2e, worst %.2e (step %d)"
+          % (rel[0], rel.max(), int(rel.argmax()) + 1))
+    assert rel[0] <= 1e-5, rel[0]
+    assert rel.max() <= LOSS_DRIFT, rel.max()
     assert abs(trainer.state()["extent"] - float(d["extent"])) <= 1e-6
     finished = trainer.finish()
     assert finished.params.shape == d["finished"].shape
