@@ -11,7 +11,9 @@ import os
 from . import _abi as A
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBRARY = os.path.join(HERE, "libpxs.so")
+# PXS_LIBRARY names another build of the same library (for example one compiled
+# with different kernel parameters); the default is the in-tree build.
+LIBRARY = os.environ.get("PXS_LIBRARY") or os.path.join(HERE, "libpxs.so")
 
 _LIB = None
 

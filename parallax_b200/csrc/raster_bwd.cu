@@ -314,10 +314,11 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
                                                dLp0[q]))));
     hi_mine = max(hi_mine, max(last0[q], last1[q]));
   }
-  float2 suffix0[NP], suffix1[NP], suffix2[NP], last_alpha[NP], lc0[NP], lc1[NP], lc2[NP];
+  // the colour composited behind the current entry (the reference's
+  // accum_rec), updated with each entry once its gradient is taken
+  float2 suffix0[NP], suffix1[NP], suffix2[NP];
 #pragma unroll
-  for (int q = 0; q < NP; ++q)
-    suffix0[q] = suffix1[q] = suffix2[q] = last_alpha[q] = lc0[q] = lc1[q] = lc2[q] = zero2;
+  for (int q = 0; q < NP; ++q) suffix0[q] = suffix1[q] = suffix2[q] = zero2;
   const int lane = lane_id(), warp = warp_id();
   const int warp_hi = __reduce_max_sync(kFull, hi_mine);
   if (threadIdx.x == 0) s_hi = info.range.x;
@@ -325,7 +326,6 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
   if (lane == 0 && warp_hi > info.range.x) atomicMax(&s_hi, warp_hi);
   __syncthreads();
   const int hi = s_hi;
-  const float2 one = make_float2(1.f, 1.f);
 
   for (int batch_end = hi; batch_end > info.range.x; batch_end -= kB) {
     const int batch_start = max(info.range.x, batch_end - kB);
@@ -405,30 +405,19 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         put(q, 6, w6.x + w6.y);
         put(q, 7, w7.x + w7.y);
         put(q, 8, w8.x + w8.y);
-        // suffix = la * lc + (1 - la) * suffix, only where this entry counts
-        const float2 la = make_float2(c0 ? last_alpha[q].x : 0.f, c1 ? last_alpha[q].y : 0.f);
-        const float2 keep = __fadd2_rn(one, make_float2(-la.x, -la.y));
-        suffix0[q] = __ffma2_rn(la, lc0[q], __fmul2_rn(keep, suffix0[q]));
-        suffix1[q] = __ffma2_rn(la, lc1[q], __fmul2_rn(keep, suffix1[q]));
-        suffix2[q] = __ffma2_rn(la, lc2[q], __fmul2_rn(keep, suffix2[q]));
-        if (c0) {
-          lc0[q].x = c.x; lc1[q].x = c.y; lc2[q].x = c.z; last_alpha[q].x = alpha.x;
-        }
-        if (c1) {
-          lc0[q].y = c.x; lc1[q].y = c.y; lc2[q].y = c.z; last_alpha[q].y = alpha.y;
-        }
+        // colour minus what lies behind (SplatRaster.cpp:399-405), then the
+        // entry joins what lies behind for the entries in front of it:
+        // suffix += alpha (colour - suffix), which leaves a pixel that does
+        // not take the entry (alpha 0) unchanged
+        const float2 d0 = __fadd2_rn(make_float2(c.x, c.x), make_float2(-suffix0[q].x, -suffix0[q].y));
+        const float2 d1 = __fadd2_rn(make_float2(c.y, c.y), make_float2(-suffix1[q].x, -suffix1[q].y));
+        const float2 d2c = __fadd2_rn(make_float2(c.z, c.z), make_float2(-suffix2[q].x, -suffix2[q].y));
         float2 dL_dalpha = __fmul2_rn(
-            __ffma2_rn(
-                __fadd2_rn(make_float2(c.z, c.z), make_float2(-suffix2[q].x, -suffix2[q].y)),
-                dLp2[q],
-                __ffma2_rn(
-                    __fadd2_rn(make_float2(c.y, c.y), make_float2(-suffix1[q].x, -suffix1[q].y)),
-                    dLp1[q],
-                    __fmul2_rn(__fadd2_rn(make_float2(c.x, c.x),
-                                          make_float2(-suffix0[q].x, -suffix0[q].y)),
-                               dLp0[q]))),
-            T[q]);
+            __ffma2_rn(d2c, dLp2[q], __ffma2_rn(d1, dLp1[q], __fmul2_rn(d0, dLp0[q]))), T[q]);
         dL_dalpha = __ffma2_rn(make_float2(-inv.x, -inv.y), bg_term[q], dL_dalpha);
+        suffix0[q] = __ffma2_rn(alpha, d0, suffix0[q]);
+        suffix1[q] = __ffma2_rn(alpha, d1, suffix1[q]);
+        suffix2[q] = __ffma2_rn(alpha, d2c, suffix2[q]);
         // the 0.99 cap flattens the gradient
         const bool t0 = c0 && r0 < kMaxAlpha, t1 = c1 && r1 < kMaxAlpha;
         if (!(t0 || t1)) continue;

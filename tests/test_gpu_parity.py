@@ -397,10 +397,12 @@ def device_buffers(arrays):
     return [torch.from_numpy(a).cuda() for a in arrays]
 
 
-def test_adam_is_bit_exact(ctx):
+@pytest.mark.parametrize("n,rest", [(4099, 15), (4096, 15), (1024, 3), (6, 0)])
+def test_adam_is_bit_exact(ctx, n, rest):
+    """Both forms of the Adam kernel: one gaussian per thread (any count) and
+    four per thread with 16-byte accesses (counts that are multiples of 4)."""
     torch = pytest.importorskip("torch")
-    rs = np.random.default_rng(5)
-    n, rest = 4099, 15
+    rs = np.random.default_rng(5 + n)
     P = px.param_count(rest)
     params = rs.normal(0, 1, (P, n)).astype(np.float32)
     grads = rs.normal(0, 1e-3, (P, n)).astype(np.float32)
