@@ -73,6 +73,9 @@ def parse_args():
     p.add_argument("--px", default="",
                    help="pixels per thread 'F,B' for compositing and its adjoint "
                         "(default: the autotuner picks)")
+    p.add_argument("--quality", action="store_true",
+                   help="train the batched and the plain form side by side for --steps steps "
+                        "and report their PSNR (c4, or c3 for the phone-shape schedule)")
     p.add_argument("--dry-run", action="store_true",
                    help="launch and rank protocol only, on CPU over gloo (no device)")
     return p.parse_args()
@@ -353,6 +356,13 @@ def run_ours(args):
         trainer._check(lib.pxs_trainer_autotune(trainer.handle, V, ids0, ct.byref(fpx),
                                                 ct.byref(bpx)))
 
+    sched = [ct.c_int32() for _ in range(4)]
+    lib.pxs_get_raster_schedule(*[ct.byref(x) for x in sched])
+    tuning = {"pixels_per_thread": {"forward": fpx.value, "backward": bpx.value},
+              "entry_batch": {"forward": sched[0].value, "backward": sched[1].value},
+              "tile_schedule": {"forward": sched[2].value, "backward": sched[3].value},
+              "schedules": "0 one CTA per tile, 1 heaviest tiles first, 2 persistent"}
+
     # warm-up: capture the graph, then once more with stage timing on
     for _ in range(max(args.warmup, 3)):
         next_batch(0)
@@ -527,7 +537,7 @@ def run_ours(args):
         "data": DATA,
         "config": workload_config(args.workload, w, V, pool),
         "parallelism": f"dp{world} over views, one GPU per rank",
-        "tuning": {"pixels_per_thread": {"forward": fpx.value, "backward": bpx.value}},
+        "tuning": tuning,
         "plain": {"ms_per_step": ms_plain,
                   "value": world * 1000.0 / ms_plain if ms_plain else None,
                   "batched_over_plain": (ms_plain / ms_batched) if ms_plain else None,
@@ -633,6 +643,85 @@ def run_multi_scene(args):
     print(json.dumps(line))
 
 
+def psnr(rendered, target):
+    """10 log10(1 / MSE) over linear RGB clamped to [0, 1]."""
+    mse = float(np.mean((np.clip(rendered, 0.0, 1.0) - target) ** 2))
+    return 10.0 * np.log10(1.0 / max(mse, 1e-20))
+
+
+def run_quality(args):
+    """Equal quality of the batched (graph-captured) form and the plain form.
+
+    c4: both forms train the C4 scene for `--steps` steps (8 views per step, the
+        benchmark's view schedule) from the same start; PSNR over the 64 pool
+        views.
+    c3: the phone-shape schedule (200k gaussians SH3, 64 cameras at 1280x720,
+        7000 iterations, densify/prune every 100 steps in [500, 5000], opacity
+        reset, SH bands unlocked every 1000): one trainer steps with
+        pxs_trainer_step (per-view kernels, host-synchronised), the other with
+        one-view graph-captured batched steps on the same schedule; final
+        gaussian counts and PSNR over the 64 training views.
+    """
+    import torch
+
+    import parallax_b200 as px
+    from parallax_b200.scenes import WORKLOADS, workload_scene
+
+    torch.cuda.set_device(0)
+    w = WORKLOADS[args.workload]
+    truth, start, views = workload_scene(args.workload)
+    lib = px.lib()
+    opts = px.RasterOptions(sh_degree=w["sh_degree"])
+    renderer = px.SplatTrainer(truth, [], px.TrainConfig(iterations=1))
+    targets = []
+    for view in views:
+        arr = np.empty(view.width * view.height * 3, dtype=np.float32)
+        cam = view.camera()
+        renderer._check(lib.pxs_trainer_render(renderer.handle, ct.byref(cam), ct.byref(opts),
+                                               arr.ctypes.data, None))
+        targets.append(np.rint(np.clip(arr, 0, 1) * 255.0).astype(np.float32) / np.float32(255))
+    renderer.close()
+    pairs = [(v.camera(), t) for v, t in zip(views, targets)]
+    if args.workload == "c4":
+        cfg = px.TrainConfig(iterations=100000, sh_degree=w["sh_degree"], sh_increase_interval=0,
+                             densify_from_iteration=10 ** 9, densify_until_iteration=10 ** 9,
+                             opacity_reset_interval=0, max_gaussians=max(600000, start.count))
+    else:
+        cfg = px.TrainConfig(iterations=args.steps, sh_degree=w["sh_degree"])
+    forms = {"batched": px.SplatTrainer(start, pairs, cfg), "plain": px.SplatTrainer(start, pairs, cfg)}
+    V, pool = w["views_per_step"], len(views)
+    t0 = time.perf_counter()
+    losses = {k: [] for k in forms}
+    for s in range(args.steps):
+        if args.workload == "c4":
+            ids = view_ids(s, V, pool)
+            losses["batched"].append(forms["batched"].step_batch(V, ids, graph=True))
+            losses["plain"].append(forms["plain"].step_views(V, ids))
+        else:
+            if not forms["plain"].step():
+                break
+            losses["plain"].append(forms["plain"].last_loss())
+            losses["batched"].append(forms["batched"].step_batch(1, None, graph=True))
+    seconds = time.perf_counter() - t0
+    result = {"quality": args.workload, "steps": args.steps, "seconds": seconds,
+              "psnr_definition": "10 log10(1/MSE), linear RGB clamped to [0,1], mean over "
+                                 f"the {pool} training views"}
+    for name, t in forms.items():
+        values = []
+        for view, target in zip(views, targets):
+            arr = np.empty(view.width * view.height * 3, dtype=np.float32)
+            cam = view.camera()
+            t._check(lib.pxs_trainer_render(t.handle, ct.byref(cam), None, arr.ctypes.data, None))
+            values.append(psnr(arr, target))
+        st = t.state()
+        result[name] = {"psnr_db": float(np.mean(values)), "gaussians": st["count"],
+                        "iteration": st["iteration"], "last_loss": st["last_loss"],
+                        "smoothed_loss": st["smoothed_loss"]}
+        t.close()
+    result["psnr_delta_db"] = result["batched"]["psnr_db"] - result["plain"]["psnr_db"]
+    print(json.dumps(result))
+
+
 def traffic_from_profiles(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -734,6 +823,8 @@ def main():
         sys.exit(spawn_ranks(args))
     if args.dry_run:
         run_dry(args)
+    elif args.quality:
+        run_quality(args)
     elif args.workload == "c5":
         run_multi_scene(args)
     else:

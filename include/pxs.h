@@ -386,12 +386,33 @@ int pxs_trainer_render(pxs_trainer* trainer, const pxs_camera* camera,
 int pxs_set_raster_config(int32_t forward_px, int32_t backward_px);
 int pxs_get_raster_config(int32_t* forward_px, int32_t* backward_px);
 
-/* The autotuner: times the compositing kernel and its adjoint with 1, 2 and
- * 4 pixels per thread on the batch of `view_ids` (NULL: the first n_views
- * views) and keeps the fastest forward + adjoint pair, timed together (the
- * two-pixel forward records which 8x8 blocks took each entry, which the
- * two-pixel adjoint uses), written to forward_px / backward_px (either may be
- * NULL). The schedule, the cloud and its gradients are not changed. */
+/* The launch shape of the two-pixel compositing kernel and of its adjoint:
+ * the tile-list entries each CTA stages per batch (64, 128 or 256; 0 keeps
+ * the current value) and how CTAs map to tiles: 0 one CTA per tile in tile
+ * order, 1 one CTA per tile with the tiles of longest lists first, 2 one
+ * persistent launch of as many CTAs as the device holds at once, taking tiles
+ * longest-list first from a device counter (-1 keeps the current value).
+ * The logical 16-pixel tiles, and so every result, stay the same: only the
+ * order in which the adjoint's atomics sum gradients changes. Process-wide,
+ * read at launch; a trainer re-captures its step graph after a change.
+ * Defaults: batches 128 / 256, schedule 0 / 0. The reference's Vulkan
+ * trainer fixes both: one workgroup per tile in tile order
+ * (VulkanSplatTrainer.cpp:570, 607; forward.comp:14, backward.comp:16). */
+int pxs_set_raster_schedule(int32_t forward_batch, int32_t backward_batch,
+                            int32_t forward_schedule, int32_t backward_schedule);
+int pxs_get_raster_schedule(int32_t* forward_batch, int32_t* backward_batch,
+                            int32_t* forward_schedule, int32_t* backward_schedule);
+
+/* The autotuner, on the batch of `view_ids` (NULL: the first n_views views):
+ * first the pixels per thread of the compositing kernel and its adjoint (1,
+ * 2 or 4 each, the pair timed together: the two-pixel forward records which
+ * 8x8 blocks took each entry, which the two-pixel adjoint uses); then, for the
+ * two-pixel forms chosen, the per-block entry batch (64 / 128 / 256) and the
+ * tile schedule (0 / 1 / 2) of each kernel, one at a time. Keeps the fastest
+ * settings (pxs_get_raster_config / pxs_get_raster_schedule read them) and
+ * writes the pixels per thread to forward_px / backward_px (either may be
+ * NULL). The schedule of training, the cloud and its gradients are not
+ * changed. */
 int pxs_trainer_autotune(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                          int32_t* forward_px, int32_t* backward_px);
 

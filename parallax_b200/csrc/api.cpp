@@ -254,6 +254,32 @@ int pxs_get_raster_config(int32_t* forward_px, int32_t* backward_px) {
   return PXS_OK;
 }
 
+int pxs_set_raster_schedule(int32_t forward_batch, int32_t backward_batch,
+                            int32_t forward_schedule, int32_t backward_schedule) {
+  auto batch_ok = [](int32_t v) { return v == 0 || v == 64 || v == 128 || v == 256; };
+  auto schedule_ok = [](int32_t v) { return v >= -1 && v <= 2; };
+  if (!batch_ok(forward_batch) || !batch_ok(backward_batch) ||
+      !schedule_ok(forward_schedule) || !schedule_ok(backward_schedule))
+    return PXS_ERR_INVALID;
+  pxs::RasterConfig& rc = pxs::raster_config();
+  if (forward_batch) rc.forward_batch = forward_batch;
+  if (backward_batch) rc.backward_batch = backward_batch;
+  if (forward_schedule >= 0) rc.forward_schedule = forward_schedule;
+  if (backward_schedule >= 0) rc.backward_schedule = backward_schedule;
+  ++rc.generation;
+  return PXS_OK;
+}
+
+int pxs_get_raster_schedule(int32_t* forward_batch, int32_t* backward_batch,
+                            int32_t* forward_schedule, int32_t* backward_schedule) {
+  const pxs::RasterConfig& rc = pxs::raster_config();
+  if (forward_batch) *forward_batch = rc.forward_batch;
+  if (backward_batch) *backward_batch = rc.backward_batch;
+  if (forward_schedule) *forward_schedule = rc.forward_schedule;
+  if (backward_schedule) *backward_schedule = rc.backward_schedule;
+  return PXS_OK;
+}
+
 const char* pxs_context_last_error(const pxs_context* ctx) {
   return ctx == nullptr ? "context is null" : ctx->error.c_str();
 }

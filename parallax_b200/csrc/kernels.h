@@ -96,14 +96,29 @@ void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint
                          cudaStream_t stream);
 
 // raster.cu
-// Pixels per thread of the compositing kernels (1, 2 or 4; TileGeom in
-// raster_common.cuh). Read at launch; set before a graph is captured.
+// Launch parameters of the compositing kernels, read at launch; set before a
+// graph is captured:
+//   pixels per thread (1, 2 or 4; TileGeom in raster_common.cuh);
+//   for the two-pixel forms, the tile-list entries staged per batch (64, 128
+//   or 256) and the CTA-to-tile schedule (TileSchedule in raster_common.cuh:
+//   0 tile order, 1 heaviest tiles first, 2 persistent, heaviest first).
 struct RasterConfig {
   int forward_px = 2;
   int backward_px = 2;
+  int forward_batch = 128;
+  int backward_batch = 256;
+  int forward_schedule = 0;
+  int backward_schedule = 0;
   int generation = 0;  // bumped on every change; captured graphs compare it
 };
 RasterConfig& raster_config();
+
+// The heaviest-first tile order of the schedules above: the tiles sorted by
+// decreasing floor(log2(list length)) (a counting sort over 32 classes; the
+// order inside a class is arbitrary and does not change any result). `work`
+// holds 64 ints.
+void launch_tile_order(const int2* ranges, int total_tiles, int* order, int* work,
+                       cudaStream_t stream);
 
 // The forward pass; with two pixels per thread and `block_bits` given it also
 // writes, per tile-list entry, a byte whose bit b is set when some pixel of
@@ -113,7 +128,8 @@ bool launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
                     cudaStream_t stream, unsigned long long* counts = nullptr,
-                    uint8_t* block_bits = nullptr);
+                    uint8_t* block_bits = nullptr, const int* tile_order = nullptr,
+                    int* ticket = nullptr);
 // The adjoint. `block_bits`, when the forward wrote them, replace the
 // geometric warp masks in the two-pixel form: a warp walks only the entries
 // one of its pixels took.
@@ -121,7 +137,8 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
                      const float4* conic_op, const float4* color, const ViewDesc* views,
                      int n_views, int total_tiles, const float* T_final, const int32_t* last,
                      const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream,
-                     const uint8_t* block_bits = nullptr);
+                     const uint8_t* block_bits = nullptr, const int* tile_order = nullptr,
+                     int* ticket = nullptr);
 
 // loss.cu
 size_t loss_smem_bytes();

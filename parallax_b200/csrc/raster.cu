@@ -8,6 +8,8 @@
 // (SplatRaster.cpp:285-310) term for term, rounded the same way (the file is
 // compiled with -fmad=false); exp is CUDA's expf, skipped only where the
 // alpha floor certainly rejects the pair (power_floor).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "raster_common.cuh"
@@ -147,19 +149,19 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
 // multiply-add per channel (fma.rn.f32x2), which differs from the separate
 // multiply and add by at most one rounding per entry. A pixel that does not
 // take an entry adds T * 0 * colour = 0.
-template <bool kCount, bool kBits>
+// kFwdBatch entries are staged per batch (RasterConfig::forward_batch: 64, 128
+// or 256; 128 by default -- a tile stops at saturation, so a smaller batch
+// stages fewer entries past it); `schedule` maps CTAs to tiles (for_each_tile).
+template <bool kCount, bool kBits, int kFwdBatch>
 __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
     k_forward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,
                  int n_views, float* __restrict__ rgb_out, float* __restrict__ T_out,
                  int32_t* __restrict__ last_out, unsigned long long* __restrict__ counts,
-                 uint8_t* __restrict__ block_bits) {
+                 uint8_t* __restrict__ block_bits, int schedule, const int* __restrict__ order,
+                 int* __restrict__ ticket, int total_tiles) {
   constexpr int kThreads = TileGeom<2>::kThreads;
-  // half the adjoint's batch: a tile stops at saturation, so a smaller batch
-  // stages fewer entries past it (the adjoint walks to each pixel's last
-  // contributor and keeps the larger batch)
-  constexpr int kFwdBatch = kBatch / 2;
   __shared__ float2 s_xy[kFwdBatch];
   __shared__ float4 s_co[kFwdBatch];
   __shared__ float4 s_col[kFwdBatch];  // r, g, b, power floor
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
   __shared__ uint8_t s_took[TileGeom<2>::kWarps][kFwdBatch];  // warp w = 8x8 block w
   __shared__ uint8_t s_list[TileGeom<2>::kWarps][kFwdBatch];  // a warp's entries of the batch
   static_assert(kFwdBatch <= 256, "batch indices are bytes");
-  const TileInfo<2> info = tile_info<2>(views, n_views, ranges);
+  for_each_tile(schedule, order, ticket, total_tiles, [&](int tile) {
+  const TileInfo<2> info = tile_info<2>(views, n_views, ranges, tile);
   const int warp = threadIdx.x >> 5;
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha, cutoff = vd.transmittance_cutoff;
@@ -306,6 +309,60 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       atomicAdd(&counts[1], contributing);
     }
   }
+  });
+}
+
+// ------------------------------------------------ heaviest-first tile order
+
+__device__ __forceinline__ int length_class(int2 r) {
+  const int len = r.y - r.x;
+  return len > 1 ? 31 - __clz(len) : 0;  // floor(log2), 0 for 0 and 1
+}
+
+// work[0..31]: tiles per length class
+__global__ void k_tile_class_counts(const int2* __restrict__ ranges, int total_tiles,
+                                    int* __restrict__ work) {
+  __shared__ int s_count[32];
+  if (threadIdx.x < 32) s_count[threadIdx.x] = 0;
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < total_tiles) atomicAdd(&s_count[length_class(ranges[t])], 1);
+  __syncthreads();
+  if (threadIdx.x < 32 && s_count[threadIdx.x] > 0) atomicAdd(&work[threadIdx.x], s_count[threadIdx.x]);
+}
+
+// work[32 + c]: where class c starts, the longest class first
+__global__ void k_tile_class_offsets(int* __restrict__ work) {
+  const int lane = threadIdx.x;  // one warp
+  const int c = 31 - lane;      // lane 0 holds the longest class
+  const int n = work[c];
+  int x = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  work[32 + c] = x - n;
+}
+
+__global__ void k_tile_class_scatter(const int2* __restrict__ ranges, int total_tiles,
+                                     int* __restrict__ work, int* __restrict__ order) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total_tiles) return;
+  order[atomicAdd(&work[32 + length_class(ranges[t])], 1)] = t;
+}
+
+void launch_tile_order(const int2* ranges, int total_tiles, int* order, int* work,
+                       cudaStream_t stream) {
+  if (total_tiles <= 0) return;
+  const int blocks = (total_tiles + 255) / 256;
+  cudaMemsetAsync(work, 0, sizeof(int) * 32, stream);
+  count_launch();
+  k_tile_class_counts<<<blocks, 256, 0, stream>>>(ranges, total_tiles, work);
+  count_launch();
+  k_tile_class_offsets<<<1, 32, 0, stream>>>(work);
+  count_launch();
+  k_tile_class_scatter<<<blocks, 256, 0, stream>>>(ranges, total_tiles, work, order);
 }
 
 namespace {
@@ -319,11 +376,56 @@ void forward_px(const int2* ranges, const uint32_t* pair_slots, const float2* xy
       ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts);
 }
 
+// The two-pixel kernel at the configured batch and schedule. The counting
+// form always runs one CTA per tile in tile order.
+template <bool kCount, bool kBits, int B>
+void forward_x2_launch(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                       const float4* conic_op, const float4* color, const ViewDesc* views,
+                       int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
+                       cudaStream_t stream, unsigned long long* counts, uint8_t* bits,
+                       const int* order, int* ticket) {
+  const RasterConfig& rc = raster_config();
+  const int schedule = (kCount || order == nullptr) ? kTileOrder : rc.forward_schedule;
+  int grid = total_tiles;
+  if (schedule == kPersistent) {
+    grid = std::min(total_tiles, resident_ctas(k_forward_x2<kCount, kBits, B>,
+                                               TileGeom<2>::kThreads));
+    cudaMemsetAsync(ticket, 0, sizeof(int), stream);
+  }
+  k_forward_x2<kCount, kBits, B><<<grid, TileGeom<2>::kThreads, 0, stream>>>(
+      ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts, bits,
+      schedule, order, ticket, total_tiles);
+}
+
+template <bool kCount>
+void forward_x2_dispatch(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                         const float4* conic_op, const float4* color, const ViewDesc* views,
+                         int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
+                         cudaStream_t stream, unsigned long long* counts, uint8_t* bits,
+                         const int* order, int* ticket) {
+#define PXS_FWD(BITS, B)                                                                    \
+  forward_x2_launch<kCount, BITS, B>(ranges, pair_slots, xy, conic_op, color, views, n_views, \
+                                     total_tiles, rgb, T, last, stream, counts, bits, order,  \
+                                     ticket)
+  const int b = raster_config().forward_batch;
+  if (bits != nullptr) {
+    if (b == 64) PXS_FWD(true, 64);
+    else if (b == 256) PXS_FWD(true, 256);
+    else PXS_FWD(true, 128);
+  } else {
+    if (b == 64) PXS_FWD(false, 64);
+    else if (b == 256) PXS_FWD(false, 256);
+    else PXS_FWD(false, 128);
+  }
+#undef PXS_FWD
+}
+
 template <bool kCount>
 void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                       const float4* conic_op, const float4* color, const ViewDesc* views,
                       int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
-                      cudaStream_t stream, unsigned long long* counts, uint8_t* bits) {
+                      cudaStream_t stream, unsigned long long* counts, uint8_t* bits,
+                      const int* order, int* ticket) {
   switch (px) {
     case 1:
       forward_px<kCount, 1>(ranges, pair_slots, xy, conic_op, color, views, n_views,
@@ -334,13 +436,9 @@ void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, co
                             total_tiles, rgb, T, last, stream, counts);
       break;
     default:
-      if (bits != nullptr)
-        k_forward_x2<kCount, true><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
-            ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts, bits);
-      else
-        k_forward_x2<kCount, false><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
-            ranges, pair_slots, xy, conic_op, color, views, n_views, rgb, T, last, counts,
-            nullptr);
+      forward_x2_dispatch<kCount>(ranges, pair_slots, xy, conic_op, color, views, n_views,
+                                  total_tiles, rgb, T, last, stream, counts, bits, order,
+                                  ticket);
   }
 }
 
@@ -349,17 +447,19 @@ void forward_dispatch(int px, const int2* ranges, const uint32_t* pair_slots, co
 bool launch_forward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                     const float4* conic_op, const float4* color, const ViewDesc* views,
                     int n_views, int total_tiles, float* rgb, float* T, int32_t* last,
-                    cudaStream_t stream, unsigned long long* counts, uint8_t* block_bits) {
+                    cudaStream_t stream, unsigned long long* counts, uint8_t* block_bits,
+                    const int* tile_order, int* ticket) {
   if (total_tiles <= 0) return false;
   count_launch();
   const int px = raster_config().forward_px;
   uint8_t* bits = (px == 1 || px == 4) ? nullptr : block_bits;
   if (counts != nullptr)
     forward_dispatch<true>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
-                           total_tiles, rgb, T, last, stream, counts, bits);
+                           total_tiles, rgb, T, last, stream, counts, bits, tile_order, ticket);
   else
     forward_dispatch<false>(px, ranges, pair_slots, xy, conic_op, color, views, n_views,
-                            total_tiles, rgb, T, last, stream, nullptr, bits);
+                            total_tiles, rgb, T, last, stream, nullptr, bits, tile_order,
+                            ticket);
   return bits != nullptr;
 }
 

@@ -13,6 +13,8 @@
 // The branch decisions (power > 0, the alpha floor, the 0.99 cap) are taken
 // with the forward kernel's exact rounding (raster_common.cuh); the gradient
 // arithmetic itself may use fused multiply-adds.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "raster_common.cuh"
@@ -253,20 +255,22 @@ __device__ __forceinline__ uint32_t mask_from_block_bits(uint32_t bits) {
 // (multiplied by 1), its suffix colour (an FMA with a zero weight) and its
 // sums are unchanged. A thread adds its pairs' contributions before the warp
 // reduction, so one reduction serves 2 NP pixels per lane.
-template <int NP>
+// kB entries are staged per batch (RasterConfig::backward_batch: 64, 128 or
+// 256 with two pixels per thread; 128 with four, where fewer threads share a
+// batch); `schedule` maps CTAs to tiles (for_each_tile).
+template <int NP, int kB>
 __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
     k_backward_pairs(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                      const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                      const float4* __restrict__ color, const ViewDesc* __restrict__ views,
                      int n_views, const float* __restrict__ T_final,
                      const int32_t* __restrict__ last_in, const float* __restrict__ dL_drgb,
-                     ScreenGrad* __restrict__ screen, const uint8_t* __restrict__ block_bits) {
+                     ScreenGrad* __restrict__ screen, const uint8_t* __restrict__ block_bits,
+                     int schedule, const int* __restrict__ order, int* __restrict__ ticket,
+                     int total_tiles) {
   constexpr int PX = 2 * NP;
   constexpr int kThreads = TileGeom<PX>::kThreads;
   constexpr int kWarps = TileGeom<PX>::kWarps;
-  // fewer threads share a batch with more pixels each: a smaller batch keeps
-  // the shared memory per warp, and so the resident warps, about the same
-  constexpr int kB = NP == 1 ? kBatch : kBatch / 2;
   __shared__ uint32_t s_slot[kB];
   __shared__ float2 s_xy[kB];
   __shared__ float4 s_co[kB];
@@ -276,7 +280,8 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
   __shared__ uint8_t s_list[kWarps][kB];  // a warp's entries of the batch
   __shared__ int s_hi;
   static_assert(kB <= 256, "batch indices are bytes");
-  const TileInfo<PX> info = tile_info<PX>(views, n_views, ranges);
+  for_each_tile(schedule, order, ticket, total_tiles, [&](int tile) {
+  const TileInfo<PX> info = tile_info<PX>(views, n_views, ranges, tile);
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha;
   const float fx = (float)info.px + 0.5f;
@@ -484,6 +489,7 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
       }
     }
   }
+  });
 }
 
 namespace {
@@ -499,11 +505,29 @@ void backward_px(const int2* ranges, const uint32_t* pair_slots, const float2* x
 
 }  // namespace
 
+template <int NP, int B>
+void backward_pairs_launch(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
+                           const float4* conic_op, const float4* color, const ViewDesc* views,
+                           int n_views, int total_tiles, const float* T_final,
+                           const int32_t* last, const float* dL_drgb, ScreenGrad* screen,
+                           cudaStream_t stream, const uint8_t* block_bits,
+                           const int* tile_order, int* ticket) {
+  const int schedule = tile_order == nullptr ? kTileOrder : raster_config().backward_schedule;
+  int grid = total_tiles;
+  if (schedule == kPersistent) {
+    grid = std::min(total_tiles, resident_ctas(k_backward_pairs<NP, B>, TileGeom<2 * NP>::kThreads));
+    cudaMemsetAsync(ticket, 0, sizeof(int), stream);
+  }
+  k_backward_pairs<NP, B><<<grid, TileGeom<2 * NP>::kThreads, 0, stream>>>(
+      ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb, screen,
+      block_bits, schedule, tile_order, ticket, total_tiles);
+}
+
 void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float2* xy,
                      const float4* conic_op, const float4* color, const ViewDesc* views,
                      int n_views, int total_tiles, const float* T_final, const int32_t* last,
                      const float* dL_drgb, ScreenGrad* screen, cudaStream_t stream,
-                     const uint8_t* block_bits) {
+                     const uint8_t* block_bits, const int* tile_order, int* ticket) {
   if (total_tiles <= 0) return;
   count_launch();
   switch (raster_config().backward_px) {
@@ -512,14 +536,21 @@ void launch_backward(const int2* ranges, const uint32_t* pair_slots, const float
                      T_final, last, dL_drgb, screen, stream);
       break;
     case 4:
-      k_backward_pairs<2><<<total_tiles, TileGeom<4>::kThreads, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
-          screen, block_bits);
+      backward_pairs_launch<2, kBatch / 2>(ranges, pair_slots, xy, conic_op, color, views,
+                                           n_views, total_tiles, T_final, last, dL_drgb,
+                                           screen, stream, block_bits, tile_order, ticket);
       break;
-    default:
-      k_backward_pairs<1><<<total_tiles, TileGeom<2>::kThreads, 0, stream>>>(
-          ranges, pair_slots, xy, conic_op, color, views, n_views, T_final, last, dL_drgb,
-          screen, block_bits);
+    default: {
+      const int b = raster_config().backward_batch;
+#define PXS_BWD(B)                                                                         \
+  backward_pairs_launch<1, B>(ranges, pair_slots, xy, conic_op, color, views, n_views,    \
+                              total_tiles, T_final, last, dL_drgb, screen, stream, block_bits, \
+                              tile_order, ticket)
+      if (b == 64) PXS_BWD(64);
+      else if (b == 128) PXS_BWD(128);
+      else PXS_BWD(256);
+#undef PXS_BWD
+    }
   }
 }
 

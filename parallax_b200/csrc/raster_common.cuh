@@ -34,9 +34,9 @@ struct TileInfo {
 
 template <int PX>
 __device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ views,
-                                                  int n_views, const int2* __restrict__ ranges) {
+                                                  int n_views, const int2* __restrict__ ranges,
+                                                  int tile) {
   TileInfo<PX> info;
-  const int tile = blockIdx.x;
   info.view = view_of_tile(views, n_views, tile);
   const ViewDesc& vd = views[info.view];
   const int local = tile - vd.tile_offset;
@@ -48,6 +48,59 @@ __device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ v
   info.py0 = info.tile_py + (w >> 1) * TileGeom<PX>::kBlockH + PX * (lane >> 3);
   info.range = ranges[tile];
   return info;
+}
+
+template <int PX>
+__device__ __forceinline__ TileInfo<PX> tile_info(const ViewDesc* __restrict__ views,
+                                                  int n_views, const int2* __restrict__ ranges) {
+  return tile_info<PX>(views, n_views, ranges, (int)blockIdx.x);
+}
+
+// CTAs of `kernel` with `threads` threads that are resident on the current
+// device at once: the grid of a persistent launch.
+template <typename Kernel>
+inline int resident_ctas(Kernel kernel, int threads) {
+  int device = 0, sms = 1, per_sm = 1;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+}
+
+// How the two-pixel compositing kernel and its adjoint map CTAs to tiles
+// (RasterConfig::forward_schedule / backward_schedule):
+//   kTileOrder   one CTA per tile, in tile order;
+//   kHeavyFirst  one CTA per tile, tiles with the longest lists first
+//                (tile = order[blockIdx.x]; the block scheduler starts
+//                CTAs roughly in index order);
+//   kPersistent  as many CTAs as fit on the device, each taking the next
+//                tile of that order from a device counter until none is left.
+enum TileSchedule { kTileOrder = 0, kHeavyFirst = 1, kPersistent = 2 };
+
+// Runs body(tile) for the tiles of this CTA under a schedule. `order` is the
+// heaviest-first tile order (schedules 1 and 2), `ticket` the counter of the
+// persistent schedule, zero at launch.
+template <typename Body>
+__device__ __forceinline__ void for_each_tile(int schedule, const int* __restrict__ order,
+                                              int* __restrict__ ticket, int total_tiles,
+                                              Body&& body) {
+  if (schedule == kTileOrder) {
+    body((int)blockIdx.x);
+    return;
+  }
+  if (schedule == kHeavyFirst) {
+    body(order[blockIdx.x]);
+    return;
+  }
+  __shared__ int s_next;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int item = s_next;
+    __syncthreads();  // every thread has read it before thread 0 takes the next
+    if (item >= total_tiles) break;
+    body(order[item]);
+  }
 }
 
 // The hardware square-root approximation (relative error about 2^-22).

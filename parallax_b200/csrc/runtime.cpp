@@ -147,6 +147,10 @@ void Frame::prepare(const ViewBatch& b, int n, int s, cudaStream_t stream) {
   transmittance.reserve(pixels);
   last.reserve(pixels);
   ranges.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  tile_order.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
+  order_work.reserve(64);
+  tickets.reserve(2);
+  order_ready = false;
   tile_counts.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
   tile_offsets.reserve(static_cast<size_t>(std::max(batch.total_tiles, 1)));
   row_ranges.reserve(static_cast<size_t>(std::max(batch.total_rows, 1)));
@@ -213,6 +217,7 @@ void Frame::project(const float* params, cudaStream_t stream, bool want_debug) {
 }
 
 int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
+  order_ready = false;  // new tile lists
   const int64_t slots = static_cast<int64_t>(V) * slot_stride;
   if (slots == 0) {
     last_pair_count = 0;
@@ -280,11 +285,24 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   return K;
 }
 
+// The heaviest-first tile order of the current lists, when a schedule wants it.
+const int* Frame::ordered_tiles(int schedule, cudaStream_t stream) {
+  if (schedule == 0) return nullptr;
+  if (!order_ready) {
+    launch_tile_order(ranges.get(), batch.total_tiles, tile_order.get(), order_work.get(),
+                      stream);
+    PXS_CUDA(cudaGetLastError());
+    order_ready = true;
+  }
+  return tile_order.get();
+}
+
 void Frame::forward(cudaStream_t stream, unsigned long long* counts) {
+  const int* order = counts ? nullptr : ordered_tiles(raster_config().forward_schedule, stream);
   have_block_bits =
       launch_forward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
                      d_views.get(), V, batch.total_tiles, rgb.get(), transmittance.get(),
-                     last.get(), stream, counts, block_bits.get());
+                     last.get(), stream, counts, block_bits.get(), order, tickets.get());
   PXS_CUDA(cudaGetLastError());
 }
 
@@ -304,9 +322,11 @@ void Frame::loss(const float* target, float ssim_weight, int mode, float* grad_o
 void Frame::backward(const float* dL_drgb, cudaStream_t stream) {
   const size_t slots = static_cast<size_t>(V) * static_cast<size_t>(slot_stride);
   PXS_CUDA(cudaMemsetAsync(screen.get(), 0, sizeof(ScreenGrad) * slots, stream));
+  const int* order = ordered_tiles(raster_config().backward_schedule, stream);
   launch_backward(ranges.get(), sorted_pair_vals, xy.get(), conic_op.get(), color.get(),
                   d_views.get(), V, batch.total_tiles, transmittance.get(), last.get(), dL_drgb,
-                  screen.get(), stream, have_block_bits ? block_bits.get() : nullptr);
+                  screen.get(), stream, have_block_bits ? block_bits.get() : nullptr, order,
+                  tickets.get() + 1);
   PXS_CUDA(cudaGetLastError());
 }
 

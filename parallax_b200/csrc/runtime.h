@@ -172,6 +172,11 @@ class Frame {
   DeviceArray<uint32_t> hist, hist_scanned;
   DeviceArray<char> scan_scratch;
   DeviceArray<int2> ranges;
+  // heaviest-first tile order (launch_tile_order) and the persistent
+  // schedule's counters (forward, adjoint)
+  DeviceArray<int32_t> tile_order, order_work, tickets;
+  bool order_ready = false;
+  const int* ordered_tiles(int schedule, cudaStream_t stream);
   DeviceArray<float> rgb, transmittance, dL;
   DeviceArray<int32_t> last;
   DeviceArray<double> loss_sums;

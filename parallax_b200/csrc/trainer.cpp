@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <numeric>
 #include <random>
 #include <string>
@@ -646,10 +647,48 @@ struct pxs_trainer {
       cudaEventDestroy(e1);
       throw;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     rc.forward_px = best_fwd;
     rc.backward_px = best_bwd;
+    // then, for the two-pixel forms, the per-block batch and the tile
+    // schedule of each kernel, one knob at a time, the others held
+    try {
+      auto tune = [&](int& knob, std::initializer_list<int> values, auto&& measure) {
+        int best_value = knob;
+        float best_ms = 0.f;
+        bool have = false;
+        for (int value : values) {
+          knob = value;
+          const float ms = measure();
+          if (!have || ms < best_ms) {
+            best_ms = ms;
+            best_value = value;
+            have = true;
+          }
+        }
+        knob = best_value;
+      };
+      auto fwd_ms = [&] { return time_ms([&] { frame.forward(stream); }); };
+      auto bwd_ms = [&] {
+        frame.forward(stream);  // block bits and the last contributors of this forward
+        return time_ms([&] { frame.backward(d_dL, stream); });
+      };
+      if (rc.forward_px == 2) {
+        tune(rc.forward_batch, {64, 128, 256}, fwd_ms);
+        tune(rc.forward_schedule, {0, 1, 2}, fwd_ms);
+      }
+      if (rc.backward_px == 2) {
+        frame.forward(stream);
+        frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
+        tune(rc.backward_batch, {64, 128, 256}, bwd_ms);
+        tune(rc.backward_schedule, {0, 1, 2}, bwd_ms);
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     ++rc.generation;
     if (forward_px) *forward_px = best_fwd;
     if (backward_px) *backward_px = best_bwd;

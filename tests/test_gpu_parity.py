@@ -347,6 +347,43 @@ def test_pixels_per_thread_variants_agree(ctx, fwd_px, bwd_px):
     assert lib.pxs_set_raster_config(3, 0) == px._abi.PXS_ERR_INVALID
 
 
+@pytest.mark.parametrize("shape", [(64, 256, 1, 1), (256, 64, 2, 2), (128, 128, 2, 1),
+                                   (128, 256, 0, 2)])
+def test_batch_and_tile_schedule_leave_results_unchanged(ctx, shape):
+    """The per-block entry batch (64 / 128 / 256) and the tile schedule (tile
+    order, heaviest first, persistent) of the two-pixel kernels change how the
+    work is cut, not what is computed: transmittance and colours identical to
+    the default launch shape, gradients within the adjoint's summation-order
+    tolerance, visible counts identical."""
+    lib = px.lib()
+    fb, bb, fs, bs = shape
+    old = [ct.c_int32() for _ in range(4)]
+    lib.pxs_get_raster_schedule(*[ct.byref(x) for x in old])
+    view, opt, cloud = make_case("random:3")
+    target = np.random.default_rng(11).uniform(0, 1, view.width * view.height * 3).astype(
+        np.float32)
+    try:
+        assert lib.pxs_set_raster_config(2, 2) == 0
+        assert lib.pxs_set_raster_schedule(128, 256, 0, 0) == 0
+        rgb0, T0 = px.render_splats(cloud, view.camera(), opt, ctx)
+        g0 = px.SplatGradients.zeros(cloud)
+        loss0 = px.render_and_accumulate(cloud, view.camera(), opt, target, 0.2, g0, ctx)
+        assert lib.pxs_set_raster_schedule(fb, bb, fs, bs) == 0
+        rgb1, T1 = px.render_splats(cloud, view.camera(), opt, ctx)
+        g1 = px.SplatGradients.zeros(cloud)
+        loss1 = px.render_and_accumulate(cloud, view.camera(), opt, target, 0.2, g1, ctx)
+    finally:
+        lib.pxs_set_raster_schedule(*[x.value for x in old])
+    assert np.array_equal(T0, T1)
+    assert np.array_equal(rgb0, rgb1)
+    assert abs(loss0 - loss1) <= 1e-6 * abs(loss0)
+    assert np.array_equal(g0.visible_count, g1.visible_count)
+    errs = grad_errors(g1.params, g0.params)
+    assert max(errs.values()) <= 1e-5, errs
+    assert lib.pxs_set_raster_schedule(100, 0, -1, -1) == px._abi.PXS_ERR_INVALID
+    assert lib.pxs_set_raster_schedule(0, 0, 3, -1) == px._abi.PXS_ERR_INVALID
+
+
 @pytest.mark.parametrize("name", ["raster_sh0.npz", "raster_sh3.npz"])
 def test_render_and_accumulate_matches_golden_reference(ctx, name):
     d, view, opt, cloud = golden_case(name)
