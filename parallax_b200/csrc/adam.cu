@@ -5,6 +5,7 @@
 // thread per gaussian so the quaternion can be renormalised in registers.
 // Compiled with -fmad=false: with IEEE division and square root the update is
 // bit-identical to the reference's for identical gradients.
+#include <tuple>
 #include <type_traits>
 
 #include "common.cuh"
@@ -106,10 +107,16 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
-// k_adam with four consecutive gaussians per thread and 16-byte loads and
-// stores, for N a multiple of 4 (every component row then starts on a 16-byte
-// boundary): element by element the same arithmetic, in the same order, so
-// the result is the same bits; a quarter of the memory instructions.
+// Adam as an elementwise pass over (task, group of four gaussians), for N a
+// multiple of 4 (every component row then starts on a 16-byte boundary): a
+// thread updates one parameter row of four consecutive gaussians with 16-byte
+// loads and stores. Task t < 6 is row t (position, log-scale); task 6 is the
+// four rotation rows together, so the quaternion is renormalised in
+// registers; tasks 7.. are rows 10.. (opacity, dc, sh_rest); with statistics
+// the last task folds this step's densify statistics into the running totals.
+// Element by element the arithmetic of k_adam, so the results are the same
+// bits; many small independent threads keep enough loads in flight to stream
+// the eight P x N arrays at close to the memory bandwidth.
 __device__ __forceinline__ void ld4(const float* base, int64_t row, int64_t n, int g4,
                                     float (&x)[4]) {
   const float4 t = reinterpret_cast<const float4*>(base + row * n)[g4];
@@ -123,92 +130,87 @@ __device__ __forceinline__ void st4(float* base, int64_t row, int64_t n, int g4,
   reinterpret_cast<float4*>(base + row * n)[g4] = make_float4(x[0], x[1], x[2], x[3]);
 }
 
-__global__ void __launch_bounds__(256, 2)
-    k_adam4(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m,
-            float* __restrict__ v, int N, int S, const StepScalars* __restrict__ scalars,
-            int zero_grads, float* __restrict__ screen_gradient,
-            int32_t* __restrict__ visible_count, float* __restrict__ acc_gradient,
-            int32_t* __restrict__ acc_views, const int32_t* __restrict__ skip,
-            const float* __restrict__ position_scale) {
+__global__ void __launch_bounds__(256)
+    k_adam_rows(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m,
+                float* __restrict__ v, int N, int S, const StepScalars* __restrict__ scalars,
+                int zero_grads, float* __restrict__ screen_gradient,
+                int32_t* __restrict__ visible_count, float* __restrict__ acc_gradient,
+                int32_t* __restrict__ acc_views, const int32_t* __restrict__ skip,
+                const float* __restrict__ position_scale) {
   const int g4 = blockIdx.x * blockDim.x + threadIdx.x;
   if (g4 >= N / 4) return;
   if (skip != nullptr && *skip != 0) return;
   const StepScalars& s = *scalars;
   const int64_t n = N;
   const int P = 14 + 3 * S;
-  float lr_position[4] = {s.lr[0], s.lr[0], s.lr[0], s.lr[0]};
-  if (position_scale != nullptr) {
-    float ps[4];
-    ld4(position_scale, 0, n, g4, ps);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) lr_position[e] = s.lr[0] * ps[e];
-  }
+  const int task = blockIdx.y;
   const float zero[4] = {0.f, 0.f, 0.f, 0.f};
-  // rows [c0, c0 + K): all loads of the group before its stores
-  auto update = [&](auto K, int c0, auto lr_of) {
-    constexpr int k = decltype(K)::value;
-    float pp[k][4], gg[k][4], mm[k][4], vv[k][4];
+  if (task == 6) {
+    float q[4][4];
 #pragma unroll
-    for (int j = 0; j < k; ++j) {
-      ld4(params, c0 + j, n, g4, pp[j]);
-      ld4(grads, c0 + j, n, g4, gg[j]);
-      ld4(m, c0 + j, n, g4, mm[j]);
-      ld4(v, c0 + j, n, g4, vv[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < k; ++j) {
+    for (int a = 0; a < 4; ++a) {
+      float pp[4], gg[4], mm[4], vv[4];
+      ld4(params, PXS_C_ROTATION + a, n, g4, pp);
+      ld4(grads, PXS_C_ROTATION + a, n, g4, gg);
+      ld4(m, PXS_C_ROTATION + a, n, g4, mm);
+      ld4(v, PXS_C_ROTATION + a, n, g4, vv);
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        pp[j][e] += adam_delta(mm[j][e], vv[j][e], gg[j][e], lr_of(c0 + j, e), s.beta1,
-                               s.beta2, s.epsilon, s.correction1, s.correction2);
-      st4(params, c0 + j, n, g4, pp[j]);
-      st4(m, c0 + j, n, g4, mm[j]);
-      st4(v, c0 + j, n, g4, vv[j]);
-      if (zero_grads) st4(grads, c0 + j, n, g4, zero);
+        q[a][e] = pp[e] + adam_delta(mm[e], vv[e], gg[e], s.lr[2], s.beta1, s.beta2, s.epsilon,
+                                     s.correction1, s.correction2);
+      st4(m, PXS_C_ROTATION + a, n, g4, mm);
+      st4(v, PXS_C_ROTATION + a, n, g4, vv);
+      if (zero_grads) st4(grads, PXS_C_ROTATION + a, n, g4, zero);
     }
-  };
-  using Three = std::integral_constant<int, 3>;
-  using Two = std::integral_constant<int, 2>;
-  using One = std::integral_constant<int, 1>;
-  update(Three{}, 0, [&](int, int e) { return lr_position[e]; });
-  update(Three{}, 3, [&](int, int) { return s.lr[1]; });
-  update(Two{}, PXS_C_OPACITY, [&](int c, int) { return c == PXS_C_OPACITY ? s.lr[3] : s.lr[4]; });
-  update(Two{}, PXS_C_DC + 1, [&](int, int) { return s.lr[4]; });
-  int c = PXS_C_SH_REST;
-  for (; c + 3 <= P; c += 3) update(Three{}, c, [&](int, int) { return s.lr[5]; });
-  for (; c < P; ++c) update(One{}, c, [&](int, int) { return s.lr[5]; });
-  float q[4][4];
+    // Quaternion::norm / normalize over (x, y, z, w) storage (SplatTrainer.cpp:247-248)
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
+    for (int e = 0; e < 4; ++e) {
+      const float w = q[0][e], x = q[1][e], y = q[2][e], z = q[3][e];
+      const float sq = (x * x + z * z) + (y * y + w * w);
+      const float norm = sqrtf(sq);
+      if (norm > 1e-6f) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) q[a][e] = q[a][e] / norm;
+      } else {
+        q[0][e] = 1.f;
+        q[1][e] = q[2][e] = q[3][e] = 0.f;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st4(params, PXS_C_ROTATION + a, n, g4, q[a]);
+    return;
+  }
+  const int row = task < 6 ? task : task + 3;  // tasks 7.. are rows 10..
+  if (row < P) {
+    float lr[4];
+    if (row < 3) {
+      float ps[4] = {1.f, 1.f, 1.f, 1.f};
+      if (position_scale != nullptr) ld4(position_scale, 0, n, g4, ps);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) lr[e] = position_scale != nullptr ? s.lr[0] * ps[e] : s.lr[0];
+    } else {
+      const float r = row < PXS_C_ROTATION ? s.lr[1]
+                      : row == PXS_C_OPACITY ? s.lr[3]
+                      : row < PXS_C_SH_REST  ? s.lr[4]
+                                             : s.lr[5];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) lr[e] = r;
+    }
     float pp[4], gg[4], mm[4], vv[4];
-    ld4(params, PXS_C_ROTATION + a, n, g4, pp);
-    ld4(grads, PXS_C_ROTATION + a, n, g4, gg);
-    ld4(m, PXS_C_ROTATION + a, n, g4, mm);
-    ld4(v, PXS_C_ROTATION + a, n, g4, vv);
+    ld4(params, row, n, g4, pp);
+    ld4(grads, row, n, g4, gg);
+    ld4(m, row, n, g4, mm);
+    ld4(v, row, n, g4, vv);
 #pragma unroll
     for (int e = 0; e < 4; ++e)
-      q[a][e] = pp[e] + adam_delta(mm[e], vv[e], gg[e], s.lr[2], s.beta1, s.beta2, s.epsilon,
-                                   s.correction1, s.correction2);
-    st4(m, PXS_C_ROTATION + a, n, g4, mm);
-    st4(v, PXS_C_ROTATION + a, n, g4, vv);
-    if (zero_grads) st4(grads, PXS_C_ROTATION + a, n, g4, zero);
+      pp[e] += adam_delta(mm[e], vv[e], gg[e], lr[e], s.beta1, s.beta2, s.epsilon,
+                          s.correction1, s.correction2);
+    st4(params, row, n, g4, pp);
+    st4(m, row, n, g4, mm);
+    st4(v, row, n, g4, vv);
+    if (zero_grads) st4(grads, row, n, g4, zero);
+    return;
   }
-  // Quaternion::norm / normalize over (x, y, z, w) storage (SplatTrainer.cpp:247-248)
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const float w = q[0][e], x = q[1][e], y = q[2][e], z = q[3][e];
-    const float sq = (x * x + z * z) + (y * y + w * w);
-    const float norm = sqrtf(sq);
-    if (norm > 1e-6f) {
-#pragma unroll
-      for (int a = 0; a < 4; ++a) q[a][e] = q[a][e] / norm;
-    } else {
-      q[0][e] = 1.f;
-      q[1][e] = q[2][e] = q[3][e] = 0.f;
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 4; ++a) st4(params, PXS_C_ROTATION + a, n, g4, q[a]);
   // accumulateStatistics (SplatTrainer.cpp:258-263), then this step's stats clear
   if (screen_gradient != nullptr) {
     float4* sg = reinterpret_cast<float4*>(screen_gradient);
@@ -236,8 +238,8 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-// Four gaussians per thread where every row (and every statistics array) is
-// 16-byte aligned, else one.
+// The elementwise form where every row (and every statistics array) is
+// 16-byte aligned, else one gaussian per thread.
 template <typename... A>
 void launch_adam_kernel(int N, const float* params, const float* grads, const float* screen,
                         const int32_t* visible, const float* acc_gradient,
@@ -249,10 +251,14 @@ void launch_adam_kernel(int N, const float* params, const float* grads, const fl
                     (acc_gradient == nullptr || (aligned(acc_gradient) && aligned(acc_views))) &&
                     (position_scale == nullptr || aligned(position_scale));
   count_launch();
-  if (wide)
-    k_adam4<<<(N / 4 + 255) / 256, 256, 0, stream>>>(args...);
-  else
+  if (wide) {
+    // tasks: rows 0-5, the rotation rows, rows 10..P-1, the statistics
+    const int S = std::get<5>(std::make_tuple(args...));
+    const int tasks = 6 + 1 + (14 + 3 * S - 10) + (screen != nullptr ? 1 : 0);
+    k_adam_rows<<<dim3((N / 4 + 255) / 256, tasks), 256, 0, stream>>>(args...);
+  } else {
     k_adam<<<(N + 255) / 256, 256, 0, stream>>>(args...);
+  }
 }
 
 void launch_adam(float* params, float* grads, float* m, float* v, int N, int S,

@@ -442,6 +442,17 @@ def oracle_loss(rendered, target, width, height, ssim_weight, want_grad=True):
     return loss, grad
 
 
+def oracle_loss_f64(rendered, target, width, height, ssim_weight):
+    """photometricLoss evaluated in double precision (the oracle's double
+    instantiation) on float images."""
+    lib = pxo()
+    lib.pxo_photometric_loss_f64.restype = ct.c_double
+    r = np.ascontiguousarray(rendered, dtype=np.float64)
+    t = np.ascontiguousarray(target, dtype=np.float64)
+    return float(lib.pxo_photometric_loss_f64(as_ptr(r), as_ptr(t), width, height,
+                                              ct.c_double(ssim_weight), None))
+
+
 def oracle_ssim(rendered, target, width, height, want_grad=True):
     grad = np.zeros_like(rendered) if want_grad else None
     s = pxo().pxo_mean_ssim_f32(as_ptr(rendered), as_ptr(target), width, height,

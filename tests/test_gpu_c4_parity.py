@@ -12,9 +12,12 @@ from its sources with IEEE arithmetic, does the same on the host:
     depth tie decides or where a decision sits within 2e-5 of its threshold
     (a branch flip, bounded);
   * in the specified order (its own projections re-sorted with equal depths by
-    gaussian index), the image must differ only by branch flips, the loss by
-    at most 1e-5 relative and the gradients by at most 1e-4 normwise per
-    parameter group, and the visible counts not at all.
+    gaussian index), the image must differ only by branch flips, the
+    gradients by at most 1e-4 normwise per parameter group, and the visible
+    counts not at all; the loss must be within 1e-5 of the reference image's
+    loss evaluated in double precision (the reference sums its 518,400-value
+    means in float, one value after another, which is itself ~5e-4 off at
+    this size; that drift is printed and bounded by 2e-3).
 
 Every count (values beyond tolerance, flips, ties) is printed per window.
 """
@@ -66,9 +69,14 @@ def c4_windows():
         ordered = O.tie_ordered(own)
         loss_i, rgb_i, g_i, s_i, v_i = O.ref_render_and_accumulate_projected(
             start.params, start.rest_per_channel, 3, view, opt, ordered, target, 0.2)
+        # the same loss in double precision: the reference accumulates its
+        # mean in float, one value after another, which over 518,400 values
+        # drifts by ~5e-4 relative; the device sums in double
+        loss64 = O.oracle_loss_f64(rgb_i, target, view.width, view.height, 0.2)
         margin, tie = O.tie_and_flip_pixels([own, ordered], cam, opt)
         runs = sum(1 for b, e in O.tie_runs(own["depth"].view(np.uint32)) if e - b > 1)
-        results[i] = dict(target=target, rgb_own=rgb_own, loss_i=loss_i, rgb_i=rgb_i,
+        results[i] = dict(target=target, rgb_own=rgb_own, loss_i=loss_i, loss64=loss64,
+                          rgb_i=rgb_i,
                           grads_i=g_i, screen_i=s_i, visible_i=v_i, margin=margin, tie=tie,
                           visible=len(own), tie_runs=runs)
 
@@ -114,13 +122,17 @@ def test_c4_window_loss_and_gradients_match_the_reference(ctx_c4, c4_windows):
         grads = px.SplatGradients.zeros(start)
         loss = px.render_and_accumulate(start, view.camera(), opt, r["target"], 0.2, grads,
                                         ctx_c4)
-        rel = abs(loss - r["loss_i"]) / abs(r["loss_i"])
+        rel = abs(loss - r["loss64"]) / abs(r["loss64"])
+        ref_rel = abs(r["loss_i"] - r["loss64"]) / abs(r["loss64"])
         errs = grad_errors(grads.params, r["grads_i"])
         screen = float(np.linalg.norm(grads.screen_gradient - r["screen_i"])
                        / max(np.linalg.norm(r["screen_i"]), 1e-30))
-        print(f"window {i}: loss {loss:.7f} (reference {r['loss_i']:.7f}, rel {rel:.2e}); "
-              f"gradient errors {errs}; screen gradient {screen:.2e}")
+        print(f"window {i}: loss {loss:.7f}; the reference's image scored in double "
+              f"{r['loss64']:.7f} (rel {rel:.2e}); the reference's own float-accumulated loss "
+              f"{r['loss_i']:.7f} (rel {ref_rel:.2e} from double); gradient errors {errs}; "
+              f"screen gradient {screen:.2e}")
         assert rel <= 1e-5, (i, rel)
+        assert ref_rel <= 2e-3, (i, ref_rel)
         assert np.array_equal(grads.visible_count, r["visible_i"]), i
         assert max(errs.values()) <= 1e-4, (i, errs)
         assert screen <= 1e-4, (i, screen)

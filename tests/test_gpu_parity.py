@@ -38,7 +38,7 @@ import parallax_b200 as px
 from parallax_b200._abi import PROJECTED_DTYPE, RasterOptions, TrainConfig
 
 # Loss drift allowed over the 60-step trainer run (relative, worst step).
-LOSS_DRIFT = 1e-3
+LOSS_DRIFT = 2e-5
 
 pytestmark = pytest.mark.gpu
 

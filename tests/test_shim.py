@@ -22,7 +22,7 @@ import oracle_lib as O
 from parallax_b200._abi import RasterOptions, TrainConfig
 
 # Loss drift allowed over the 60-step trainer run (relative, worst step).
-LOSS_DRIFT = 1e-3
+LOSS_DRIFT = 2e-5
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
