@@ -41,11 +41,54 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// A frame already at the target size (downscaleToWidth returns it unchanged,
+// ImageIo.cpp:301-303): every byte divided by 255, 16 bytes per thread with
+// 16-byte loads and stores. The same float as k_downscale writes for a box of
+// one pixel.
+__global__ void __launch_bounds__(256)
+    k_bytes_to_linear16(const uint4* __restrict__ src, float4* __restrict__ out, int64_t n16) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n16) return;
+  const uint4 w = src[i];
+  const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t v = words[k];
+    out[i * 4 + k] = make_float4((float)(v & 0xFFu) / 255.f, (float)((v >> 8) & 0xFFu) / 255.f,
+                                 (float)((v >> 16) & 0xFFu) / 255.f, (float)(v >> 24) / 255.f);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_bytes_to_linear(const uint8_t* __restrict__ src, uint8_t* __restrict__ out_bytes,
+                      float* __restrict__ out_linear, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t b = src[i];
+  if (out_bytes != nullptr) out_bytes[i] = b;
+  if (out_linear != nullptr) out_linear[i] = (float)b / 255.f;
+}
+
 void launch_downscale(const uint8_t* src, int width, int height, int out_width, int out_height,
                       uint8_t* out_bytes, float* out_linear, cudaStream_t stream) {
   const int64_t n = (int64_t)out_width * out_height;
   if (n <= 0) return;
   count_launch();
+  if (out_width == width && out_height == height) {
+    const int64_t bytes = n * 3;
+    const bool wide = out_bytes == nullptr && out_linear != nullptr && bytes % 16 == 0 &&
+                      (reinterpret_cast<uintptr_t>(src) & 15u) == 0 &&
+                      (reinterpret_cast<uintptr_t>(out_linear) & 15u) == 0;
+    if (wide) {
+      const int64_t n16 = bytes / 16;
+      k_bytes_to_linear16<<<(unsigned)((n16 + 255) / 256), 256, 0, stream>>>(
+          reinterpret_cast<const uint4*>(src), reinterpret_cast<float4*>(out_linear), n16);
+    } else {
+      k_bytes_to_linear<<<(unsigned)((bytes + 255) / 256), 256, 0, stream>>>(src, out_bytes,
+                                                                             out_linear, bytes);
+    }
+    return;
+  }
   k_downscale<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(src, width, height, out_width,
                                                                out_height, out_bytes, out_linear);
 }

@@ -125,3 +125,25 @@ def test_staged_frames_train_like_ingested_frames():
         staged.stage_images([0], [np.zeros(640 * 400 * 3, np.uint8)], [(640, 400)])
     for t in (sync, staged):
         t.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width,height", [(320, 240), (161, 97)])
+def test_frames_at_the_view_size_convert_like_the_host(width, height):
+    """Frames already at the view's size (downscaleToWidth returns them as
+    they are): the device's byte-to-float pass (16 bytes per thread where the
+    sizes allow, one otherwise) gives the host's frame / 255 exactly."""
+    params, rest = O.random_cloud(73, 800, 0)
+    cloud = px.GaussianCloud(params, 0, rest)
+    views = O.orbit_views(2, width, height, seed=6)
+    rs = np.random.default_rng(width)
+    frames = [rs.integers(0, 256, width * height * 3, dtype=np.uint8) for _ in range(2)]
+    t = px.SplatTrainer(cloud, [(v.camera(), np.zeros(width * height * 3, np.float32))
+                                for v in views], px.TrainConfig(iterations=2))
+    t.ingest_images([0, 1], frames, [(width, height)] * 2)
+    a = px.SplatTrainer(cloud, [(v.camera(), f.astype(np.float32) / np.float32(255.0))
+                                for v, f in zip(views, frames)], px.TrainConfig(iterations=2))
+    assert t.step_batch(2, [0, 1]) == a.step_batch(2, [0, 1])
+    assert np.array_equal(t.cloud_params().view(np.uint32), a.cloud_params().view(np.uint32))
+    for x in (t, a):
+        x.close()
