@@ -511,13 +511,17 @@ int pxs_trainer_ingest_images(pxs_trainer* trainer, int32_t n, const int32_t* vi
 
 /* The same ingest, asynchronous, for a training loop that feeds each step's
  * frames from host memory: the frames are copied to the device on the
- * trainer's own copy stream while the current step runs, into one of two
- * staging buffers, and are downscaled and converted into the views' training
- * images (as pxs_trainer_ingest_images does) at the start of the next call
- * that steps or replaces images (pxs_trainer_step, _step_batch, _step_views,
- * _accumulate, _ingest_images, _set_images, or another stage call, which
- * applies the earlier set first). The frames must stay valid and unchanged
- * until that call returns; page-locked frames let the copy overlap the step.
+ * trainer's own copy stream, into one of two staging buffers, while the
+ * steps before the one that needs them run, and are downscaled and converted
+ * into the views' training images (as pxs_trainer_ingest_images does) by the
+ * first step call (pxs_trainer_step, _step_batch, _step_views, _accumulate)
+ * whose views include one of theirs; _ingest_images, _set_images and
+ * _autotune apply every staged set first, and a stage call with both buffers
+ * busy applies the older set. Sets take effect in the order they were
+ * staged. So a loop that stages step s+1's frames and then runs step s
+ * copies them while step s runs. The frames must stay valid and unchanged
+ * until the call that applies them returns; page-locked frames let the copy
+ * overlap the step.
  * No reference counterpart: the reference converts on the host before
  * training (Pipeline.cpp:1892-1917). */
 int pxs_trainer_stage_images(pxs_trainer* trainer, int32_t n, const int32_t* view_ids,

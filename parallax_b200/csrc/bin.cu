@@ -131,10 +131,11 @@ __device__ __forceinline__ void warp_range_counts(const uint32_t (&range)[K], in
 }
 
 // Per-warp column counts of one chunk of row records into s_cnt
-// [kWarps][max_tiles_x] (zeroed by the caller); lanes prefetch their records'
-// rects first.
+// [kWarps][max_tiles_x] (zeroed by the caller). Each record's column range
+// was stored beside it when the records were written (rec_xr), so it is read
+// with the record instead of gathered through the record's slot.
 __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32_t* __restrict__ rec_slots,
-                                                    const uint2* __restrict__ rect, int max_tiles_x,
+                                                    const uint32_t* __restrict__ rec_xr, int max_tiles_x,
                                                     int tiles_x, int32_t* s_cnt,
                                                     uint32_t (&slot)[kPerLane],
                                                     uint32_t (&xr)[kPerLane]) {
@@ -147,7 +148,7 @@ __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32
     xr[k] = 1u;  // x0 = 1 > x1 = 0: covers nothing
     if (rec < ch.z) {
       slot[k] = rec_slots[rec];
-      xr[k] = rect[slot[k]].x;
+      xr[k] = rec_xr[rec];
     }
   }
   warp_range_counts(xr, tiles_x, s_cnt + w * max_tiles_x);
@@ -156,7 +157,7 @@ __device__ __forceinline__ void chunk_column_counts(const int4& ch, const uint32
 // Per chunk: how many of its records cover each column.
 __global__ void __launch_bounds__(kWarps * 32)
     k_chunk_counts(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
-                   const uint32_t* __restrict__ rec_slots, const uint2* __restrict__ rect,
+                   const uint32_t* __restrict__ rec_slots, const uint32_t* __restrict__ rec_xr,
                    const ViewDesc* __restrict__ views, int n_views, int max_tiles_x,
                    int32_t* __restrict__ chunk_counts) {
   extern __shared__ int32_t s_cnt[];  // [kWarps][max_tiles_x]
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     s_cnt[(i / tiles_x) * max_tiles_x + (i % tiles_x)] = 0;
   __syncthreads();
   uint32_t slot[kPerLane], xr[kPerLane];
-  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, s_cnt, slot, xr);
+  chunk_column_counts(ch, rec_slots, rec_xr, max_tiles_x, tiles_x, s_cnt, slot, xr);
   __syncthreads();
   for (int c = threadIdx.x; c < tiles_x; c += blockDim.x) {
     int total = 0;
@@ -306,7 +307,9 @@ __device__ __forceinline__ void warp_range_expand(const uint32_t (&range)[K],
                                                   uint32_t* bitmap, bool staged,
                                                   uint32_t* stage, const int32_t* col_start,
                                                   const int64_t* col_dst, int64_t capacity,
-                                                  uint32_t* __restrict__ out) {
+                                                  uint32_t* __restrict__ out,
+                                                  const uint32_t (*extra)[K] = nullptr,
+                                                  uint32_t* __restrict__ out_extra = nullptr) {
   const int lane = lane_id();
   const unsigned lt = lanemask_lt();
 #pragma unroll
@@ -320,7 +323,10 @@ __device__ __forceinline__ void warp_range_expand(const uint32_t (&range)[K],
         stage[pos] = payload[k];
       } else {
         const int64_t dst = col_dst[c] + (pos - col_start[c]);
-        if (dst < capacity) out[dst] = payload[k];
+        if (dst < capacity) {
+          out[dst] = payload[k];
+          if (out_extra != nullptr) out_extra[dst] = (*extra)[k];
+        }
       }
     }
     __syncwarp();
@@ -339,16 +345,23 @@ __device__ __forceinline__ void warp_range_expand(const uint32_t (&range)[K],
 
 // The staged pairs out to their lists: one warp per column, consecutive
 // entries per lane.
+// With `rect` and `out_x` the records also get their slot's column range.
 __device__ __forceinline__ void copy_out_staged(int extent, const int32_t* col_count,
                                                 const int32_t* col_start,
                                                 const int64_t* col_dst, const uint32_t* stage,
-                                                int64_t capacity, uint32_t* __restrict__ out) {
+                                                int64_t capacity, uint32_t* __restrict__ out,
+                                                const uint2* __restrict__ rect = nullptr,
+                                                uint32_t* __restrict__ out_x = nullptr) {
   const int w = warp_id(), lane = lane_id();
   for (int c = w; c < extent; c += kWarps) {
     const int n = col_count[c], src = col_start[c];
     const int64_t dst = col_dst[c];  // >= 0: offsets and bases are counts
     for (int i = lane; i < n; i += 32)
-      if (dst + i < capacity) out[dst + i] = stage[src + i];
+      if (dst + i < capacity) {
+        const uint32_t v = stage[src + i];
+        out[dst + i] = v;
+        if (out_x != nullptr) out_x[dst + i] = rect[v].x;
+      }
   }
 }
 
@@ -384,7 +397,7 @@ __device__ __forceinline__ ExpandSmem expand_smem(int32_t* s_mem, int max_extent
 // the stage holds stores them straight into the lists instead.
 __global__ void __launch_bounds__(kWarps * 32)
     k_chunk_expand(const int4* __restrict__ chunks, const int32_t* __restrict__ n_chunks,
-                   const uint32_t* __restrict__ rec_slots, const uint2* __restrict__ rect,
+                   const uint32_t* __restrict__ rec_slots, const uint32_t* __restrict__ rec_xr,
                    const ViewDesc* __restrict__ views, int n_views, int max_tiles_x,
                    const int32_t* __restrict__ chunk_base,
                    const int64_t* __restrict__ tile_offsets, int64_t capacity,
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   __syncthreads();
   uint32_t slot[kPerLane], xr[kPerLane];
-  chunk_column_counts(ch, rec_slots, rect, max_tiles_x, tiles_x, e.cnt, slot, xr);
+  chunk_column_counts(ch, rec_slots, rec_xr, max_tiles_x, tiles_x, e.cnt, slot, xr);
   __syncthreads();
   const int64_t tile0 = (int64_t)vd.tile_offset + (int64_t)(ch.x - vd.row_offset) * tiles_x;
   const bool staged = chunk_layout(
@@ -484,7 +497,7 @@ __global__ void __launch_bounds__(kWarps * 32)
                       const int32_t* __restrict__ tile_count, const uint2* __restrict__ rect,
                       const ViewDesc* __restrict__ views, int64_t slot_stride, int cpv,
                       int max_tiles_y, const int64_t* __restrict__ offsets, int64_t capacity,
-                      uint32_t* __restrict__ rec_slots) {
+                      uint32_t* __restrict__ rec_slots, uint32_t* __restrict__ rec_xr) {
   extern __shared__ __align__(16) int32_t s_mem[];
   __shared__ int s_warp[kWarps];
   const int v = blockIdx.x / cpv, c = blockIdx.x % cpv;
@@ -505,11 +518,17 @@ __global__ void __launch_bounds__(kWarps * 32)
   const bool staged = chunk_layout(
       e.cnt, max_tiles_y, tiles_y, kStage, s_warp, e.col_count, e.col_start, e.col_dst,
       [&](int y) { return offsets[(int64_t)(vd.row_offset + y) * cpv + c]; });
+  uint32_t xr[kSlotPerLane];  // the column ranges, written beside the records
+  if (!staged) {
+#pragma unroll
+    for (int k = 0; k < kSlotPerLane; ++k) xr[k] = rect[slot[k]].x;
+  }
   warp_range_expand(yr, slot, e.cnt + w * max_tiles_y, e.bitmap + w * max_tiles_y, staged,
-                    e.stage, e.col_start, e.col_dst, capacity, rec_slots);
+                    e.stage, e.col_start, e.col_dst, capacity, rec_slots, &xr, rec_xr);
   if (!staged) return;
   __syncthreads();
-  copy_out_staged(tiles_y, e.col_count, e.col_start, e.col_dst, e.stage, capacity, rec_slots);
+  copy_out_staged(tiles_y, e.col_count, e.col_start, e.col_dst, e.stage, capacity, rec_slots,
+                  rect, rec_xr);
 }
 
 // row_ranges[r] = [offsets[r * cpv], offsets[(r + 1) * cpv]) (the total for the
@@ -566,13 +585,14 @@ void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_co
 void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
-                            int64_t capacity, uint32_t* rec_slots, cudaStream_t stream) {
+                            int64_t capacity, uint32_t* rec_slots, uint32_t* rec_xr,
+                            cudaStream_t stream) {
   const int cpv = slot_chunks_per_view(slot_stride);
   if (n_views <= 0 || cpv <= 0) return;
   count_launch();
   k_slot_row_expand<<<(unsigned)(n_views * cpv), kWarps * 32, chunk_expand_smem(max_tiles_y),
                       stream>>>(sorted_slots, tile_count, rect, views, slot_stride, cpv,
-                                max_tiles_y, offsets, capacity, rec_slots);
+                                max_tiles_y, offsets, capacity, rec_slots, rec_xr);
 }
 
 void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int cpv,
@@ -586,7 +606,7 @@ void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int c
 
 int64_t max_row_chunks(int64_t records, int total_rows) { return records / kChunk + total_rows + 1; }
 
-void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint32_t* rec_xr,
                        const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
                        int64_t max_chunks, int4* chunks, int32_t* n_chunks,
                        int32_t* chunk_counts, int32_t* chunk_base, int32_t* tile_counts,
@@ -596,7 +616,7 @@ void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const 
   k_row_chunks<<<1, 1024, 0, stream>>>(row_ranges, total_rows, (int)max_chunks, chunks, n_chunks);
   count_launch();
   k_chunk_counts<<<(unsigned)max_chunks, kWarps * 32, chunk_counts_smem(max_tiles_x), stream>>>(
-      chunks, n_chunks, rec_slots, rect, views, n_views, max_tiles_x, chunk_counts);
+      chunks, n_chunks, rec_slots, rec_xr, views, n_views, max_tiles_x, chunk_counts);
   count_launch();
   k_row_tiles<<<total_rows, 256, 0, stream>>>(chunks, n_chunks, views, n_views, max_tiles_x,
                                               chunk_counts, chunk_base, tile_counts);
@@ -612,14 +632,14 @@ void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, i
 }
 
 void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint32_t* rec_slots,
-                         const uint2* rect, const ViewDesc* views, int n_views, int max_tiles_x,
+                         const uint32_t* rec_xr, const ViewDesc* views, int n_views, int max_tiles_x,
                          int64_t max_chunks, const int32_t* chunk_base,
                          const int64_t* tile_offsets, int64_t capacity, uint32_t* tile_slots,
                          cudaStream_t stream) {
   if (max_chunks <= 0) return;
   count_launch();
   k_chunk_expand<<<(unsigned)max_chunks, kWarps * 32, chunk_expand_smem(max_tiles_x), stream>>>(
-      chunks, n_chunks, rec_slots, rect, views, n_views, max_tiles_x, chunk_base, tile_offsets,
+      chunks, n_chunks, rec_slots, rec_xr, views, n_views, max_tiles_x, chunk_base, tile_offsets,
       capacity, tile_slots);
 }
 

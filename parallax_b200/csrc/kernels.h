@@ -72,7 +72,8 @@ void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_co
 void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
-                            int64_t capacity, uint32_t* rec_slots, cudaStream_t stream);
+                            int64_t capacity, uint32_t* rec_slots, uint32_t* rec_xr,
+                            cudaStream_t stream);
 // Per-row record ranges from the chunk offsets, clamped to the capacity
 // (records past it raise the overflow flag).
 void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int cpv,
@@ -81,7 +82,7 @@ void launch_row_ranges_from_chunks(const int64_t* offsets, int total_rows, int c
 // Upper bound on the number of row chunks for `records` records.
 int64_t max_row_chunks(int64_t records, int total_rows);
 // Chunk table, per-chunk column counts, per-chunk bases and tile lengths.
-void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint2* rect,
+void launch_tile_lists(const int2* row_ranges, const uint32_t* rec_slots, const uint32_t* rec_xr,
                        const ViewDesc* views, int n_views, int total_rows, int max_tiles_x,
                        int64_t max_chunks, int4* chunks, int32_t* n_chunks,
                        int32_t* chunk_counts, int32_t* chunk_base, int32_t* tile_counts,
@@ -90,7 +91,7 @@ void launch_ranges_from_offsets(const int32_t* counts, const int64_t* offsets, i
                                 int64_t capacity, int2* ranges, int32_t* overflow,
                                 cudaStream_t stream);
 void launch_chunk_expand(const int4* chunks, const int32_t* n_chunks, const uint32_t* rec_slots,
-                         const uint2* rect, const ViewDesc* views, int n_views, int max_tiles_x,
+                         const uint32_t* rec_xr, const ViewDesc* views, int n_views, int max_tiles_x,
                          int64_t max_chunks, const int32_t* chunk_base,
                          const int64_t* tile_offsets, int64_t capacity, uint32_t* tile_slots,
                          cudaStream_t stream);

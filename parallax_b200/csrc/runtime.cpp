@@ -187,6 +187,7 @@ void Frame::reserve_records(int64_t capacity) {
   if (capacity <= record_capacity && rec_vals.get() != nullptr) return;
   const size_t cap = static_cast<size_t>(std::max<int64_t>(capacity, 1));
   rec_vals.reserve(cap);
+  rec_xr.reserve(cap);
   record_capacity = static_cast<int64_t>(cap);
   ensure_chunks();
 }
@@ -254,14 +255,14 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
   launch_slot_row_expand(v, tile_count.get(), rect.get(), d_views.get(), V, slot_stride,
                          batch.max_tiles_y, row_chunk_offsets.get(), record_capacity,
-                         rec_vals.get(), stream);
+                         rec_vals.get(), rec_xr.get(), stream);
   launch_row_ranges_from_chunks(row_chunk_offsets.get(), batch.total_rows, cpv,
                                 d_total_records.get(), record_capacity, row_ranges.get(),
                                 overflow.get(), stream);
   const uint32_t* rv = rec_vals.get();
   // 4. tile lengths from chunked rows, their offsets, then the lists themselves
   ensure_chunks();
-  launch_tile_lists(row_ranges.get(), rv, rect.get(), d_views.get(), V, batch.total_rows,
+  launch_tile_lists(row_ranges.get(), rv, rec_xr.get(), d_views.get(), V, batch.total_rows,
                     batch.max_tiles_x, max_chunks, chunks.get(), n_chunks.get(),
                     chunk_counts.get(), chunk_base.get(), tile_counts.get(), stream);
   exclusive_scan_i32_to_i64(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
@@ -277,7 +278,7 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   }
   launch_ranges_from_offsets(tile_counts.get(), tile_offsets.get(), batch.total_tiles,
                              pair_capacity, ranges.get(), overflow.get(), stream);
-  launch_chunk_expand(chunks.get(), n_chunks.get(), rv, rect.get(), d_views.get(), V,
+  launch_chunk_expand(chunks.get(), n_chunks.get(), rv, rec_xr.get(), d_views.get(), V,
                       batch.max_tiles_x, max_chunks, chunk_base.get(), tile_offsets.get(),
                       pair_capacity, tile_slots.get(), stream);
   sorted_pair_vals = tile_slots.get();

@@ -159,6 +159,7 @@ class Frame {
   DeviceArray<int32_t> row_chunk_counts;
   DeviceArray<int64_t> row_chunk_offsets, d_total_pairs, d_total_records;
   DeviceArray<uint32_t> rec_vals;  // tile-row records (slot ids) by row, near to far
+  DeviceArray<uint32_t> rec_xr;    // each record's tile-column range (x0 | x1 << 16)
   DeviceArray<int2> row_ranges;
   DeviceArray<int32_t> tile_counts, chunk_counts, chunk_base, n_chunks;
   DeviceArray<int4> chunks;

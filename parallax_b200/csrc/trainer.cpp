@@ -81,21 +81,25 @@ struct pxs_trainer {
   DeviceArray<float> images;
   DeviceArray<uint8_t> ingest_in;  // staging for 8-bit frames
 
-  // Frames staged for a coming step (pxs_trainer_stage_images): copied to
-  // the device on copy_stream, into one of two staging buffers, while the
-  // current step runs, then converted into the image store on `stream` before
-  // the next step's kernels. A staging buffer is refilled only after the
-  // conversion that read it (consumed_event) has run.
+  // Frames staged for coming steps (pxs_trainer_stage_images): each set is
+  // copied to the device on copy_stream into one of two staging buffers while
+  // the steps before it run, and converted into the image store on `stream`
+  // by the first step that uses one of its views (older sets first, so images
+  // are replaced in the order they were staged). A staging buffer is refilled
+  // only after the conversion that read it (consumed_event) has run.
   struct StagedFrame {
     int view, width, height, out_width, out_height;
     size_t offset;
+  };
+  struct StagedSet {
+    int slot;
+    std::vector<StagedFrame> frames;
   };
   cudaStream_t copy_stream = nullptr;
   DeviceArray<uint8_t> stage_buf[2];
   cudaEvent_t staged_event[2] = {}, consumed_event[2] = {};
   bool consumed_recorded[2] = {false, false};
-  std::vector<StagedFrame> pending;
-  int pending_slot = -1, next_slot = 0;
+  std::vector<StagedSet> pending;  // oldest first, at most two
 
   int iteration = 0;
   float extent = 1.f, last_loss = 0.f, smoothed_loss = 0.f;
@@ -306,22 +310,37 @@ struct pxs_trainer {
 
   // ---------------------------------------------------------- staged ingest
 
-  // Enqueues, on `stream`, the conversion of the staged frames into the
-  // image store, after their copy; the staging buffer is then free to refill.
-  void consume_staged() {
-    if (pending_slot < 0) return;
-    const int k = pending_slot;
-    PXS_CUDA(cudaStreamWaitEvent(stream, staged_event[k], 0));
-    for (const StagedFrame& f : pending) {
-      pxs::launch_downscale(stage_buf[k].get() + f.offset, f.width, f.height, f.out_width,
-                            f.out_height, nullptr,
-                            images.get() + image_offset[static_cast<size_t>(f.view)] * 3, stream);
-      PXS_CUDA(cudaGetLastError());
+  // Enqueues, on `stream`, the conversion of the oldest `count` staged sets
+  // into the image store, each after its copy; their buffers are then free.
+  void convert_staged(size_t count) {
+    for (size_t i = 0; i < count && i < pending.size(); ++i) {
+      const StagedSet& set = pending[i];
+      const int k = set.slot;
+      PXS_CUDA(cudaStreamWaitEvent(stream, staged_event[k], 0));
+      for (const StagedFrame& f : set.frames) {
+        pxs::launch_downscale(stage_buf[k].get() + f.offset, f.width, f.height, f.out_width,
+                              f.out_height, nullptr,
+                              images.get() + image_offset[static_cast<size_t>(f.view)] * 3,
+                              stream);
+        PXS_CUDA(cudaGetLastError());
+      }
+      PXS_CUDA(cudaEventRecord(consumed_event[k], stream));
+      consumed_recorded[k] = true;
     }
-    PXS_CUDA(cudaEventRecord(consumed_event[k], stream));
-    consumed_recorded[k] = true;
-    pending.clear();
-    pending_slot = -1;
+    pending.erase(pending.begin(), pending.begin() + std::min(count, pending.size()));
+  }
+
+  // Every staged set, before images are replaced another way.
+  void consume_staged() { convert_staged(pending.size()); }
+
+  // The staged sets a step over `views` needs: up to the newest set holding
+  // one of them (older sets first). Sets for later steps stay in flight.
+  void consume_staged_for(const std::vector<int>& views) {
+    size_t need = 0;
+    for (size_t i = 0; i < pending.size(); ++i)
+      for (const StagedFrame& f : pending[i].frames)
+        if (std::find(views.begin(), views.end(), f.view) != views.end()) need = i + 1;
+    convert_staged(need);
   }
 
   void stage_frames(int n, const int32_t* ids, const uint8_t* const* frames,
@@ -343,8 +362,6 @@ struct pxs_trainer {
       staged.push_back({id, widths[i], heights[i], w, h, total});
       total += (bytes + 255) / 256 * 256;
     }
-    // frames staged earlier take effect first
-    consume_staged();
     if (staged.empty()) return;
     if (copy_stream == nullptr) {
       PXS_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
@@ -353,8 +370,10 @@ struct pxs_trainer {
         PXS_CUDA(cudaEventCreateWithFlags(&consumed_event[k], cudaEventDisableTiming));
       }
     }
-    const int k = next_slot;
-    next_slot ^= 1;
+    // both buffers hold sets no step has used yet: the older one takes effect
+    // now, which frees its buffer
+    if (pending.size() == 2) convert_staged(1);
+    const int k = pending.empty() ? 0 : 1 - pending.front().slot;
     if (total > stage_buf[k].capacity()) {
       // grown only when both streams are idle
       PXS_CUDA(cudaStreamSynchronize(stream));
@@ -370,8 +389,7 @@ struct pxs_trainer {
                                cudaMemcpyHostToDevice, copy_stream));
     }
     PXS_CUDA(cudaEventRecord(staged_event[k], copy_stream));
-    pending = std::move(staged);
-    pending_slot = k;
+    pending.push_back({k, std::move(staged)});
   }
 
   // ---------------------------------------------------------- steps
@@ -388,8 +406,8 @@ struct pxs_trainer {
   // SplatTrainer::step (SplatTrainer.cpp:326-362): one view, synchronised.
   bool step() {
     if (schedule_done()) return false;
-    consume_staged();
     const int id = next_view();
+    consume_staged_for({id});
     const pxs::ViewBatch b = batch_for({id});
     frame.prepare(b, N, S, stream);
     frame.project(params.get(), stream);
@@ -411,7 +429,6 @@ struct pxs_trainer {
   }
 
   std::vector<int> take_views(int n_views, const int32_t* ids) {
-    consume_staged();
     std::vector<int> out;
     for (int i = 0; i < n_views; ++i) {
       const int id = ids != nullptr ? ids[i] : next_view();
@@ -419,6 +436,7 @@ struct pxs_trainer {
         throw Error(PXS_ERR_INVALID, "view id out of range");
       out.push_back(id);
     }
+    consume_staged_for(out);
     return out;
   }
 
@@ -594,6 +612,7 @@ struct pxs_trainer {
   // batch of views and keeps the fastest forward + backward pair.
   // The schedule, the parameters and the gradients are left as they were.
   void autotune(int n_views, const int32_t* ids, int* forward_px, int* backward_px) {
+    consume_staged();  // the loss reads the training images
     std::vector<int> views;
     for (int i = 0; i < n_views; ++i) {
       const int id = ids != nullptr ? ids[i] : i % static_cast<int>(cameras.size());

