@@ -483,6 +483,43 @@ def oracle_render_and_accumulate(params, rest, sh_degree, cam, opt, target, ssim
     return loss, grads, screen, visible
 
 
+def oracle_gradient_f64_in_order(params, rest, sh_degree, cam, opt, order, target,
+                                 ssim_weight):
+    """The loss gradient evaluated in double precision (the oracle's double
+    instantiation of projection, compositing, loss and backward) over the
+    splats of `order` (gaussian indices, near to far, as a float projection
+    listed them) in that order: the same entries and tie order as the float
+    computation, without its rounding. Returns (loss, grads64)."""
+    lib = pxo()
+    lib.pxo_project_f64.restype = ct.c_int32
+    lib.pxo_photometric_loss_f64.restype = ct.c_double
+    n = params.shape[1]
+    p64 = np.ascontiguousarray(params, dtype=np.float64)
+    out = np.zeros(max(n, 1), dtype=PROJECTED_F64_DTYPE)
+    count = lib.pxo_project_f64(as_ptr(p64), n, rest, sh_degree, ct.byref(cam), ct.byref(opt),
+                                as_ptr(out))
+    proj = out[:count]
+    where = np.full(n, -1, dtype=np.int64)
+    where[proj["index"]] = np.arange(count)
+    pick = where[np.asarray(order)]
+    listed = np.ascontiguousarray(proj[pick[pick >= 0]])
+    pixels = cam.width * cam.height
+    rgb = np.zeros(pixels * 3, dtype=np.float64)
+    lib.pxo_rasterize_f64(as_ptr(listed), len(listed), ct.byref(cam), ct.byref(opt),
+                          as_ptr(rgb), None)
+    t64 = np.ascontiguousarray(target, dtype=np.float64)
+    dL = np.zeros(pixels * 3, dtype=np.float64)
+    loss = lib.pxo_photometric_loss_f64(as_ptr(rgb), as_ptr(t64), cam.width, cam.height,
+                                        ct.c_double(ssim_weight), as_ptr(dL))
+    grads = np.zeros_like(p64)
+    screen = np.zeros(n, dtype=np.float64)
+    visible = np.zeros(n, dtype=np.int32)
+    lib.pxo_backward_f64(as_ptr(p64), n, rest, sh_degree, ct.byref(cam), ct.byref(opt),
+                         as_ptr(listed), len(listed), as_ptr(rgb), as_ptr(dL), as_ptr(grads),
+                         as_ptr(screen), as_ptr(visible))
+    return float(loss), grads
+
+
 def oracle_objective_f64(params64, rest, sh_degree, cam, opt, target64, ssim_weight):
     return pxo().pxo_objective_f64(as_ptr(params64), params64.shape[1], rest, sh_degree,
                                    ct.byref(cam), ct.byref(opt), as_ptr(target64),

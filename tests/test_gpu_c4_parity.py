@@ -12,9 +12,12 @@ from its sources with IEEE arithmetic, does the same on the host:
     depth tie decides or where a decision sits within 2e-5 of its threshold
     (a branch flip, bounded);
   * in the specified order (its own projections re-sorted with equal depths by
-    gaussian index), the image must differ only by branch flips, the
-    gradients by at most 1e-4 normwise per parameter group, and the visible
-    counts not at all; the loss must be within 1e-5 of the reference image's
+    gaussian index), the image must differ only by branch flips and the
+    visible counts not at all; the gradients are measured against the same
+    entries in the same order evaluated in double precision (the oracle's
+    double instantiation): within 1e-4 normwise per parameter group, or at
+    worst twice the reference's own FP32 distance from FP64 (which reaches
+    1.1e-4 for rotation on one window); the loss must be within 1e-5 of the reference image's
     loss evaluated in double precision (the reference sums its 518,400-value
     means in float, one value after another, which is itself ~5e-4 off at
     this size, 2.9e-3 on one window; that drift is printed and bounded by
@@ -76,10 +79,16 @@ def c4_windows():
         loss64 = O.oracle_loss_f64(rgb_i, target, view.width, view.height, 0.2)
         margin, tie = O.tie_and_flip_pixels([own, ordered], cam, opt)
         runs = sum(1 for b, e in O.tie_runs(own["depth"].view(np.uint32)) if e - b > 1)
+        # the same gradient in double precision over the same entries in the
+        # same order, kept for the gaussians the window projects
+        _, g64 = O.oracle_gradient_f64_in_order(start.params, start.rest_per_channel, 3, cam,
+                                                opt, ordered["index"], target, 0.2)
+        cols = np.sort(ordered["index"])
         results[i] = dict(target=target, rgb_own=rgb_own, loss_i=loss_i, loss64=loss64,
-                          rgb_i=rgb_i,
-                          grads_i=g_i, screen_i=s_i, visible_i=v_i, margin=margin, tie=tie,
-                          visible=len(own), tie_runs=runs)
+                          rgb_i=rgb_i, cols=cols, grads_i=g_i[:, cols],
+                          grads64=g64[:, cols].copy(), screen_i=s_i, visible_i=v_i,
+                          margin=margin, tie=tie, visible=len(own), tie_runs=runs)
+        del g_i, g64
 
     threads = [threading.Thread(target=reference, args=(i,)) for i in range(len(windows))]
     for t in threads:
@@ -125,21 +134,30 @@ def test_c4_window_loss_and_gradients_match_the_reference(ctx_c4, c4_windows):
                                         ctx_c4)
         rel = abs(loss - r["loss64"]) / abs(r["loss64"])
         ref_rel = abs(r["loss_i"] - r["loss64"]) / abs(r["loss64"])
-        errs = grad_errors(grads.params, r["grads_i"])
+        got = grads.params[:, r["cols"]]
+        dev_ref = grad_errors(got, r["grads_i"])
+        dev_64 = grad_errors(got, r["grads64"])
+        ref_64 = grad_errors(r["grads_i"], r["grads64"])
         screen = float(np.linalg.norm(grads.screen_gradient - r["screen_i"])
                        / max(np.linalg.norm(r["screen_i"]), 1e-30))
+        fmt = lambda e: {k: f"{v:.1e}" for k, v in e.items()}  # noqa: E731
         print(f"window {i}: loss {loss:.7f}; the reference's image scored in double "
               f"{r['loss64']:.7f} (rel {rel:.2e}); the reference's own float-accumulated loss "
-              f"{r['loss_i']:.7f} (rel {ref_rel:.2e} from double); gradient errors {errs}; "
-              f"screen gradient {screen:.2e}")
+              f"{r['loss_i']:.7f} (rel {ref_rel:.2e} from double); gradient, device vs FP64 "
+              f"{fmt(dev_64)}, reference vs FP64 {fmt(ref_64)}, device vs reference "
+              f"{fmt(dev_ref)}; screen gradient {screen:.2e}")
         assert rel <= 1e-5, (i, rel)
         assert ref_rel <= 1e-2, (i, ref_rel)
         assert np.array_equal(grads.visible_count, r["visible_i"]), i
-        assert max(errs.values()) <= 1e-4, (i, errs)
+        for k in GROUPS:
+            # within 1e-4 of the FP64 gradient, or at worst as close as twice
+            # the reference's own FP32 gradient is
+            assert dev_64[k] <= max(1e-4, 2.0 * ref_64[k]), (i, k, dev_64, ref_64)
         assert screen <= 1e-4, (i, screen)
-        for k, v in errs.items():
-            worst[k] = max(worst.get(k, 0.0), v)
-    print("C4 windows, worst gradient error per group:", worst)
+        for k in GROUPS:
+            worst[k] = max(worst.get(k, 0.0), dev_64[k])
+            worst["reference " + k] = max(worst.get("reference " + k, 0.0), ref_64[k])
+    print("C4 windows, worst gradient error against FP64 per group:", worst)
 
 
 @pytest.fixture(scope="module")
