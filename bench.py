@@ -362,6 +362,10 @@ def run_ours(args):
               "entry_batch": {"forward": sched[0].value, "backward": sched[1].value},
               "tile_schedule": {"forward": sched[2].value, "backward": sched[3].value},
               "schedules": "0 one CTA per tile, 1 heaviest tiles first, 2 persistent"}
+    if not args.px:
+        report = ct.create_string_buffer(8192)
+        trainer._check(lib.pxs_trainer_autotune_report(trainer.handle, report, 8192))
+        tuning["measured"] = [ln for ln in report.value.decode().splitlines() if ln]
 
     # warm-up: capture the graph, then once more with stage timing on
     for _ in range(max(args.warmup, 3)):

@@ -415,6 +415,9 @@ int pxs_get_raster_schedule(int32_t* forward_batch, int32_t* backward_batch,
  * changed. */
 int pxs_trainer_autotune(pxs_trainer* trainer, int32_t n_views, const int32_t* view_ids,
                          int32_t* forward_px, int32_t* backward_px);
+/* The last autotune's measurements, one line per candidate (mean time per
+ * launch), into `text` (truncated to `capacity`). */
+int pxs_trainer_autotune_report(pxs_trainer* trainer, char* text, size_t capacity);
 
 /* Measures this device's FP32 FMA throughput (TFLOP/s) with a microkernel:
  * the roofline denominator of the FP32-bound compositing kernels. */

@@ -74,6 +74,7 @@ def _declare(lib: ct.CDLL) -> None:
         "pxs_set_raster_config": (ct.c_int, [_i32, _i32]),
         "pxs_get_raster_config": (ct.c_int, [_vp, _vp]),
         "pxs_set_raster_schedule": (ct.c_int, [_i32, _i32, _i32, _i32]),
+        "pxs_trainer_autotune_report": (ct.c_int, [_vp, ct.c_char_p, ct.c_size_t]),
         "pxs_get_raster_schedule": (ct.c_int, [_vp, _vp, _vp, _vp]),
         "pxs_trainer_autotune": (ct.c_int, [_vp, _i32, _vp, _vp, _vp]),
         "pxs_trainer_accumulate": (ct.c_int, [_vp, _i32, _vp, _i32, _vp]),

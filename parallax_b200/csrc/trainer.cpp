@@ -120,6 +120,7 @@ struct pxs_trainer {
   pxs::DensifyWork dwork;
   DeviceArray<pxs::StepScalars> scalars;
   DeviceArray<float> dL, loss_acc;
+  std::string tune_log;       // the autotuner's timings, one line per candidate
   pxs::GraphState graph;      // the batched step
   pxs::GraphState graph_acc;  // its data-parallel accumulate half
   bool pending_apply = false;
@@ -613,6 +614,7 @@ struct pxs_trainer {
   // The schedule, the parameters and the gradients are left as they were.
   void autotune(int n_views, const int32_t* ids, int* forward_px, int* backward_px) {
     consume_staged();  // the loss reads the training images
+    tune_log.clear();
     std::vector<int> views;
     for (int i = 0; i < n_views; ++i) {
       const int id = ids != nullptr ? ids[i] : i % static_cast<int>(cameras.size());
@@ -652,7 +654,11 @@ struct pxs_trainer {
         frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
         for (int bpx : candidates) {
           rc.backward_px = bpx;
-          const float ms = f_ms + time_ms([&] { frame.backward(d_dL, stream); });
+          const float b_ms = time_ms([&] { frame.backward(d_dL, stream); });
+          const float ms = f_ms + b_ms;
+          tune_log += "pixels per thread " + std::to_string(fpx) + "/" + std::to_string(bpx) +
+                      ": forward " + std::to_string(f_ms / 3.f) + " ms, adjoint " +
+                      std::to_string(b_ms / 3.f) + " ms\n";
           if (!have_best || ms < best) {
             best = ms;
             best_fwd = fpx;
@@ -671,13 +677,16 @@ struct pxs_trainer {
     // then, for the two-pixel forms, the per-block batch and the tile
     // schedule of each kernel, one knob at a time, the others held
     try {
-      auto tune = [&](int& knob, std::initializer_list<int> values, auto&& measure) {
+      auto tune = [&](const char* what, int& knob, std::initializer_list<int> values,
+                      auto&& measure) {
         int best_value = knob;
         float best_ms = 0.f;
         bool have = false;
         for (int value : values) {
           knob = value;
           const float ms = measure();
+          tune_log += std::string(what) + " " + std::to_string(value) + ": " +
+                      std::to_string(ms / 3.f) + " ms\n";
           if (!have || ms < best_ms) {
             best_ms = ms;
             best_value = value;
@@ -692,14 +701,14 @@ struct pxs_trainer {
         return time_ms([&] { frame.backward(d_dL, stream); });
       };
       if (rc.forward_px == 2) {
-        tune(rc.forward_batch, {64, 128, 256}, fwd_ms);
-        tune(rc.forward_schedule, {0, 1, 2}, fwd_ms);
+        tune("forward batch", rc.forward_batch, {64, 128, 256}, fwd_ms);
+        tune("forward schedule", rc.forward_schedule, {0, 1, 2}, fwd_ms);
       }
       if (rc.backward_px == 2) {
         frame.forward(stream);
         frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
-        tune(rc.backward_batch, {64, 128, 256}, bwd_ms);
-        tune(rc.backward_schedule, {0, 1, 2}, bwd_ms);
+        tune("adjoint batch", rc.backward_batch, {64, 128, 256}, bwd_ms);
+        tune("adjoint schedule", rc.backward_schedule, {0, 1, 2}, bwd_ms);
       }
     } catch (...) {
       cudaEventDestroy(e0);
@@ -957,6 +966,14 @@ int pxs_trainer_autotune(pxs_trainer* t, int32_t n_views, const int32_t* view_id
     t->autotune(n_views, view_ids, &f, &b);
     if (forward_px) *forward_px = f;
     if (backward_px) *backward_px = b;
+  });
+}
+
+int pxs_trainer_autotune_report(pxs_trainer* t, char* text, size_t capacity) {
+  return guarded(t, [&] {
+    if (text == nullptr || capacity == 0) throw Error(PXS_ERR_INVALID, "no buffer");
+    std::strncpy(text, t->tune_log.c_str(), capacity - 1);
+    text[capacity - 1] = '\0';
   });
 }
 
