@@ -114,6 +114,51 @@ def ties_case():
           "pairs", len(entries))
 
 
+def c1_run_case():
+    """The plain CPU-runnable configuration end to end under the reference's own
+    trainer (SplatTrainer.cpp:326-362): 20k gaussians SH0 (start cloud seed 2),
+    16 cameras on a radius-3 sphere at 320x240 (seed 3), targets rendered by
+    the reference from the truth cloud (seed 1) and quantised to 8-bit frames
+    (stored, and trained on as frame / 255), 200 iterations of one view, the
+    reference's default schedule otherwise. Records the loss of every
+    iteration and the final cloud's PSNR over the 16 views."""
+    import parallax_b200 as px
+    from parallax_b200.scenes import workload_scene
+
+    truth, start, views = workload_scene("c1")
+    opt = RasterOptions(sh_degree=0)
+    oviews = [O.View(tuple(v.K), v.width, v.height, np.asarray(v.R), np.asarray(v.t))
+              for v in views]
+    frames = []
+    for v in oviews:
+        rgb, _ = O.ref_render(truth.params, 0, 0, v, opt)
+        frames.append(np.rint(np.clip(rgb, 0, 1) * 255.0).astype(np.uint8))
+    images = [f.astype(np.float32) / np.float32(255.0) for f in frames]
+    cfg = TrainConfig(iterations=200, sh_degree=0)
+    trainer = O.RefTrainer(start.params, 0, 0, oviews, images, cfg)
+    losses = []
+    while trainer.step():
+        losses.append(trainer.state()["last_loss"])
+    final = trainer.cloud()
+    psnr = []
+    for v, im in zip(oviews, images):
+        rgb, _ = O.ref_render(final, 0, 0, v, opt)
+        mse = float(np.mean((np.clip(rgb, 0, 1).astype(np.float64) - im) ** 2))
+        psnr.append(10.0 * np.log10(1.0 / mse))
+    arrays = {}
+    for i, v in enumerate(oviews):
+        for k, a in view_arrays(v).items():
+            arrays[f"view{i}_{k}"] = a
+    # the start cloud is not stored: pxs_synthetic_cloud(2, 20000, 0) regenerates
+    # it (tests/test_ref_bench.py pins that generator to the reference's Rng)
+    np.savez_compressed(os.path.join(HERE, "c1_run.npz"), frames=np.stack(frames),
+                        losses=np.array(losses, np.float32), psnr=np.array(psnr),
+                        n_views=np.int32(len(oviews)), **arrays)
+    print("c1 run: final loss", losses[-1], "mean PSNR", float(np.mean(psnr)), "count",
+          final.shape[1])
+    assert px is not None
+
+
 def densify_case():
     params, rest = O.random_cloud(21, 600, 1, log_scale_mean=-3.0)
     rs = np.random.default_rng(22)
@@ -171,10 +216,14 @@ def main():
     if sys.argv[1:] == ["ties"]:
         ties_case()
         return
+    if sys.argv[1:] == ["c1"]:
+        c1_run_case()
+        return
     assert O.ref_available("ieee"), "oracle/_ref/libpxref_ieee.so is required"
     raster_case("raster_sh0", 0, 700, 64, 48, seed=31)
     raster_case("raster_sh3", 3, 500, 48, 40, seed=32, background=(0.2, 0.3, 0.4))
     ties_case()
+    c1_run_case()
     densify_case()
     trainer_case()
 
