@@ -200,9 +200,10 @@ def test_c1_trains_like_the_reference_trainer():
     views at 320x240, 200 iterations of one view, the reference's default
     schedule) against the reference's own SplatTrainer run stored in
     tests/golden/c1_run.npz: the same view order, the first step's loss
-    within 1e-5, the loss curve within the drift printed below, and the final
-    PSNR within 0.05 dB of the reference's, view by view and on average. The
-    engine's SplatTrainer on the CUDA backend (the shim) is held to the same."""
+    within 1e-4 (the reference's own float-summation drift), the whole loss
+    curve within 1e-3, and the final PSNR within 0.05 dB of the reference's,
+    view by view and on average. The engine's SplatTrainer on the CUDA
+    backend (the shim) is held to the same."""
     d, views, images = _c1_run()
     start = px.synthetic_cloud(2, 20000, 0)
     cfg = TrainConfig(iterations=200, sh_degree=0)
@@ -230,7 +231,12 @@ def test_c1_trains_like_the_reference_trainer():
               f"(reference {ref_losses[-1]:.6f}); PSNR {psnr.mean():.4f} dB "
               f"(reference {ref_psnr.mean():.4f} dB), worst view difference "
               f"{np.abs(psnr - ref_psnr).max():.4f} dB")
-        assert rel[0] <= 1e-5, (name, rel[0])
+        # The reference adds its 230,400 L1 terms and 76,800 SSIM terms into a
+        # float one by one (photometricLoss); at this size that sum drifts by a
+        # few 1e-5 from the exact one (2.7e-5 measured at the first step). The
+        # device sums in double; its loss is held to 1e-5 of an FP64 evaluation
+        # in the parity tests.
+        assert rel[0] <= 1e-4, (name, rel[0])
         assert rel.max() <= 1e-3, (name, rel.max())
         assert abs(psnr.mean() - ref_psnr.mean()) <= 0.05, name
         assert np.abs(psnr - ref_psnr).max() <= 0.05, name
