@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as ct
+import datetime
 import json
 import os
 import statistics
@@ -152,23 +153,48 @@ def dist_env():
 
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock and throttle-reason samples every 50 ms. `start` waits
+    for the first sample, so that the sampler is running before the timed
+    region opens; `mark` brackets the timed region, and `stop` keeps the
+    samples whose timestamps fall inside it (the nearest one when the region
+    is shorter than the interval)."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
+        self.window = None
 
-    def start(self):
+    def start(self, wait_s: float = 10.0):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.file,
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        deadline = time.time() + wait_s
+        while time.time() < deadline and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.02)
+
+    def mark(self, t_begin: float, t_end: float):
+        self.window = (t_begin, t_end)
+
+    @staticmethod
+    def _time_of(stamp: str):
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(stamp, fmt).timestamp()
+            except ValueError:
+                pass
+        return None
 
     def stop(self):
         if self.proc is not None:
@@ -182,18 +208,27 @@ class ClockSampler:
         with open(self.file.name) as f:
             for line in f:
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if len(parts) >= 10:
                     rows.append(parts)
         os.unlink(self.file.name)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        kept = rows
+        if self.window is not None:
+            t0, t1 = self.window
+            stamped = [(self._time_of(r[0]), r) for r in rows]
+            inside = [r for t, r in stamped if t is not None and t0 <= t <= t1]
+            if inside:
+                kept = inside
+            else:
+                timed = [(abs(t - 0.5 * (t0 + t1)), r) for t, r in stamped if t is not None]
+                kept = [min(timed, key=lambda x: x[0])[1]] if timed else rows[-1:]
+        sm = [float(r[2]) for r in kept if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in kept if r[3].replace(".", "").isdigit()]
+        reasons = sorted({self.REASONS[i] for r in kept for i in range(4) if r[6 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(kept), "interval_ms": 50}
 
 
 # ------------------------------------------------------ reference CPU trainer
@@ -376,7 +411,9 @@ def run_ours(args):
 
     clocks = ClockSampler(local)
     clocks.start()
+    t_begin = time.time()
     ms_batched = timed(next_batch, args.steps)
+    clocks.mark(t_begin, time.time())
     clock_info = clocks.stop()
 
     stage_ms = (ct.c_float * len(STAGES))()
