@@ -600,6 +600,63 @@ def test_batched_and_graph_steps_match_the_plain_multi_view_step():
     assert np.abs(p0 - p1).max() <= 1e-4 and np.abs(p1 - p2).max() <= 1e-4
 
 
+def test_a_batch_with_views_that_see_nothing():
+    """A view whose camera faces away from the cloud projects no slot, builds
+    empty tile lists and renders the background. Mixed into a batch with
+    views that see the cloud, the batched and graph steps still match the
+    plain per-view step; a batch of such views alone has a zero gradient, so
+    Adam leaves every parameter exactly where it was (m = v = 0 give a zero
+    update, SplatTrainer.cpp:56-65)."""
+    params, rest = O.random_cloud(71, 20000, 3, log_scale_mean=-4.0)
+    truth, _ = O.random_cloud(72, 20000, 3, log_scale_mean=-4.0)
+    seeing = O.orbit_views(3, 160, 120, seed=8)
+    away = []
+    for eye in ([0.0, 0.0, -3.0], [3.0, 0.5, 0.0]):
+        eye = np.array(eye)
+        R = O.look_at(eye, eye * 3.0)  # looking outward: the cloud is behind
+        away.append(O.View(seeing[0].K, 96, 64, R, -R @ eye))
+    views = seeing + away
+    opt = RasterOptions(sh_degree=3)
+    images = [px.render_splats(px.GaussianCloud(truth, 3, rest), v.camera(), opt)[0]
+              for v in views]
+    for v, im in zip(away, images[3:]):
+        assert len(px.project_splats(px.GaussianCloud(params, 3, rest), v.camera(), opt)) == 0
+        assert np.allclose(im, 0.0)  # the default background is black
+    cfg = TrainConfig(iterations=100, sh_degree=3, sh_increase_interval=0,
+                      densify_from_iteration=1000, densify_until_iteration=1000)
+    pairs = [(v.camera(), im) for v, im in zip(views, images)]
+    results = []
+    for mode in ("plain", "batched", "graph"):
+        t = px.SplatTrainer(px.GaussianCloud(params, 3, rest), pairs, cfg)
+        losses = []
+        for sel in ([0, 3, 1, 4], [4, 2, 3]):
+            if mode == "plain":
+                losses.append(t.step_views(len(sel), sel))
+            else:
+                losses.append(t.step_batch(len(sel), sel, graph=(mode == "graph")))
+        results.append((losses, t.cloud_params()))
+        t.close()
+    (l0, p0), (l1, p1), (l2, p2) = results
+    assert np.allclose(l0, l1, rtol=1e-5) and np.allclose(l0, l2, rtol=1e-5)
+    assert np.abs(p0 - p1).max() <= 1e-4 and np.abs(p1 - p2).max() <= 1e-4
+    # only views that see nothing: black against black (L1 0, SSIM 1) and no
+    # parameter moves; the quaternion rows are renormalised by every step
+    # (SplatTrainer.cpp:247-248), which may move their last bit
+    rot = slice(6, 10)
+    for graph in (False, True):
+        t = px.SplatTrainer(px.GaussianCloud(params, 3, rest), pairs, cfg)
+        before = t.cloud_params()
+        loss = t.step_batch(2, [3, 4], graph=graph)
+        after = t.cloud_params()
+        assert abs(loss) <= 1e-6
+        keep = np.ones(after.shape[0], bool)
+        keep[rot] = False
+        assert np.array_equal(after[keep], before[keep])
+        assert np.abs(after[rot] - before[rot]).max() <= 1e-6
+        assert t.state()["iteration"] == 1
+        t.close()
+
+
 def test_a_graph_step_whose_tile_lists_overflow_is_redone():
     """The unsynchronised step runs with the pair and record capacities learned
     on its first batch (with headroom). A later batch with many more tile pairs
