@@ -78,6 +78,7 @@ struct pxs_trainer {
 
   std::vector<pxs_camera> cameras;
   std::vector<int64_t> image_offset;  // first pixel of each view in `images`
+  bool uniform_views = true;          // every view has the same size
   DeviceArray<float> images;
   DeviceArray<uint8_t> ingest_in;  // staging for 8-bit frames
 
@@ -123,10 +124,12 @@ struct pxs_trainer {
   std::string tune_log;       // the autotuner's timings, one line per candidate
   pxs::GraphState graph;      // the batched step
   pxs::GraphState graph_acc;  // its data-parallel accumulate half
+  pxs::GraphState graph_one;  // the one-view step (step())
   bool pending_apply = false;
   int generation = 0;  // bumped whenever a state buffer is reallocated
   float* host_loss = nullptr;     // pinned
   int32_t* host_overflow = nullptr;
+  int64_t* host_pairs = nullptr;  // pinned: the last batched step's pair count
 
   // stage timing: events recorded between the stages of the batched step
   // (captured as event nodes when the step is a graph)
@@ -143,6 +146,7 @@ struct pxs_trainer {
     if (copy_stream) cudaStreamSynchronize(copy_stream);
     graph.reset();
     graph_acc.reset();
+    graph_one.reset();
     for (int k = 0; k < 2; ++k) {
       if (staged_event[k]) cudaEventDestroy(staged_event[k]);
       if (consumed_event[k]) cudaEventDestroy(consumed_event[k]);
@@ -152,6 +156,7 @@ struct pxs_trainer {
       if (e) cudaEventDestroy(e);
     if (host_loss) cudaFreeHost(host_loss);
     if (host_overflow) cudaFreeHost(host_overflow);
+    if (host_pairs) cudaFreeHost(host_pairs);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -405,25 +410,14 @@ struct pxs_trainer {
   }
 
   // SplatTrainer::step (SplatTrainer.cpp:326-362): one view, synchronised.
+  // The batched step over that one view: its pair and record buffers are
+  // sized once with headroom (no host round trip inside the step) and, when
+  // every view has the same size, the step is one replay of its own graph.
   bool step() {
     if (schedule_done()) return false;
     const int id = next_view();
     consume_staged_for({id});
-    const pxs::ViewBatch b = batch_for({id});
-    frame.prepare(b, N, S, stream);
-    frame.project(params.get(), stream);
-    frame.bin(true, stream);
-    frame.forward(stream);
-    float* d_dL = dL.reserve(static_cast<size_t>(b.total_pixels) * 3 + 1);
-    frame.loss(images.get(), cfg.ssim_weight, 0, d_dL, stream);
-    frame.backward(d_dL, stream);
-    frame.param_grads(params.get(), d_grads(), d_screen(), visible_count.get(),
-                      stream);
-    PXS_CUDA(cudaMemcpyAsync(host_loss, frame.loss_total.get(), sizeof(float),
-                             cudaMemcpyDeviceToHost, stream));
-    upload_scalars();
-    adam();
-    PXS_CUDA(cudaStreamSynchronize(stream));
+    run_batch({id}, uniform_views, true, graph_one);
     record_loss(*host_loss);
     after_step();
     return true;
@@ -530,6 +524,8 @@ struct pxs_trainer {
                              cudaMemcpyDeviceToHost, stream));
     PXS_CUDA(cudaMemcpyAsync(host_overflow, frame.overflow.get(), sizeof(int32_t),
                              cudaMemcpyDeviceToHost, stream));
+    PXS_CUDA(cudaMemcpyAsync(host_pairs, frame.d_total_pairs.get(), sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, stream));
   }
 
   // Runs the batched body for `views`, replayed from `g` when use_graph, and
@@ -593,8 +589,7 @@ struct pxs_trainer {
       PXS_CUDA(cudaStreamSynchronize(stream));
       if (*host_overflow == 0) {
         collect_timing();
-        PXS_CUDA(cudaMemcpy(&last_pairs, frame.d_total_pairs.get(), sizeof(int64_t),
-                            cudaMemcpyDeviceToHost));
+        last_pairs = *host_pairs;
         return;
       }
       // the pairs did not fit: nothing of this step counts; grow and redo
@@ -835,6 +830,8 @@ int pxs_trainer_create(const pxs_train_config* config, const pxs_cloud* initial,
     PXS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&t->host_loss), sizeof(float)));
     PXS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&t->host_overflow), sizeof(int32_t)));
     *t->host_overflow = 0;
+    PXS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&t->host_pairs), sizeof(int64_t)));
+    *t->host_pairs = 0;
     t->cfg = *config;
     t->N = initial->count;
     t->S = S;
@@ -851,6 +848,9 @@ int pxs_trainer_create(const pxs_train_config* config, const pxs_cloud* initial,
     PXS_CUDA(cudaMemsetAsync(t->v.get(), 0, std::max<size_t>(values, 1) * sizeof(float), t->stream));
     t->resize_state();
     t->cameras.assign(cameras, cameras + n_views);
+    for (int v = 1; v < n_views; ++v)
+      if (cameras[v].width != cameras[0].width || cameras[v].height != cameras[0].height)
+        t->uniform_views = false;
     int64_t total = 0;
     for (int v = 0; v < n_views; ++v) {
       t->image_offset.push_back(total);
@@ -994,6 +994,7 @@ int pxs_trainer_render(pxs_trainer* t, const pxs_camera* camera,
     const pxs::ViewBatch b = pxs::make_batch(camera, 1, opt, t->cloud_sh);
     t->graph.reset();  // the frame's buffers may be resized
     t->graph_acc.reset();
+    t->graph_one.reset();
     t->frame.prepare(b, t->N, t->S, t->stream);
     t->frame.project(t->params.get(), t->stream);
     t->frame.bin(true, t->stream);
