@@ -699,9 +699,10 @@ def run_quality(args):
     c3: the phone-shape schedule (200k gaussians SH3, 64 cameras at 1280x720,
         7000 iterations, densify/prune every 100 steps in [500, 5000], opacity
         reset, SH bands unlocked every 1000): one trainer steps with
-        pxs_trainer_step (per-view kernels, host-synchronised), the other with
-        one-view graph-captured batched steps on the same schedule; final
-        gaussian counts and PSNR over the 64 training views.
+        pxs_trainer_step_views over one view (per-view kernels, host-
+        synchronised), the other with one-view graph-captured batched steps on
+        the same schedule; final gaussian counts and PSNR over the 64 training
+        views.
     """
     import torch
 
@@ -739,9 +740,9 @@ def run_quality(args):
             losses["batched"].append(forms["batched"].step_batch(V, ids, graph=True))
             losses["plain"].append(forms["plain"].step_views(V, ids))
         else:
-            if not forms["plain"].step():
+            if forms["plain"].state()["iteration"] >= cfg.iterations:
                 break
-            losses["plain"].append(forms["plain"].last_loss())
+            losses["plain"].append(forms["plain"].step_views(1))
             losses["batched"].append(forms["batched"].step_batch(1, None, graph=True))
     seconds = time.perf_counter() - t0
     result = {"quality": args.workload, "steps": args.steps, "seconds": seconds,
