@@ -306,7 +306,10 @@ void pxs_trainer_destroy(pxs_trainer* trainer);
 const char* pxs_trainer_last_error(const pxs_trainer* trainer);
 
 /* SplatTrainer::step (SplatTrainer.cpp:326-362): one iteration on the next
- * view. `stepped` is 0 once the schedule is finished. */
+ * view. `stepped` is 0 once the schedule is finished. It runs the batched
+ * step over that one view: no host round trip inside the step, and one
+ * replay of a captured graph when all the trainer's views share a size
+ * (pxs_trainer_step_views runs the plain per-view sequence instead). */
 int pxs_trainer_step(pxs_trainer* trainer, int32_t* stepped);
 
 /* SplatTrainer::train (SplatTrainer.cpp:364-376). `completed` is 0 when the
