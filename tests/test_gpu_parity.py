@@ -600,6 +600,44 @@ def test_batched_and_graph_steps_match_the_plain_multi_view_step():
     assert np.abs(p0 - p1).max() <= 1e-4 and np.abs(p1 - p2).max() <= 1e-4
 
 
+def test_one_view_steps_over_views_of_different_sizes():
+    """pxs_trainer_step runs the batched step over its one view, sized with
+    headroom from the first view it meets; with views of two sizes it runs
+    without a captured graph, and a large view after small ones overflows
+    the learned pair buffers, so that step is redone with larger ones. Step
+    by step it matches the plain per-view step (pxs_trainer_step_views over
+    the same view), up to the order in which the adjoint's atomics add."""
+    params, rest = O.random_cloud(91, 20000, 3, log_scale_mean=-3.0)
+    truth, _ = O.random_cloud(92, 20000, 3, log_scale_mean=-3.0)
+    small = O.orbit_views(4, 96, 72, seed=10)
+    large = O.orbit_views(2, 320, 240, radius=2.2, seed=11)
+    views = small + large
+    opt = RasterOptions(sh_degree=3)
+    images = [px.render_splats(px.GaussianCloud(truth, 3, rest), v.camera(), opt)[0]
+              for v in views]
+    cfg = TrainConfig(iterations=12, sh_degree=3, sh_increase_interval=0,
+                      densify_from_iteration=1000, densify_until_iteration=1000)
+    pairs = [(v.camera(), im) for v, im in zip(views, images)]
+    one = px.SplatTrainer(px.GaussianCloud(params, 3, rest), pairs, cfg)
+    plain = px.SplatTrainer(px.GaussianCloud(params, 3, rest), pairs, cfg)
+    lib = px.lib()
+    la, lb, step_pairs = [], [], []
+    while one.step():
+        la.append(one.last_loss())
+        lb.append(plain.step_views(1))  # the same shuffled view: the same schedule
+        k, launches = ct.c_int64(), ct.c_int64()
+        one._check(lib.pxs_trainer_step_info(one.handle, ct.byref(k), ct.byref(launches)))
+        step_pairs.append(k.value)
+    assert len(la) == 12
+    assert one.state()["iteration"] == plain.state()["iteration"] == 12
+    assert np.allclose(la, lb, rtol=1e-5)
+    assert np.abs(one.cloud_params() - plain.cloud_params()).max() <= 1e-4
+    # the large views list several times the small views' pairs
+    assert max(step_pairs) > 3 * min(step_pairs)
+    one.close()
+    plain.close()
+
+
 def test_a_batch_with_views_that_see_nothing():
     """A view whose camera faces away from the cloud projects no slot, builds
     empty tile lists and renders the background. Mixed into a batch with
