@@ -196,7 +196,7 @@ int pxs_gpu_availability(int32_t* available, char* device_name, size_t device_na
   }
   copy_string(prop.name, device_name, device_name_len);
   if (prop.major != 10 || prop.minor != 0) {
-    copy_string("this build needs an sm_100 (B200-class) device; found sm_" +
+    copy_string("the library is compiled for sm_100a (B200-class) devices; found sm_" +
                     std::to_string(prop.major) + std::to_string(prop.minor),
                 reason, reason_len);
     return PXS_OK;
