@@ -445,29 +445,40 @@ constexpr int kSlotChunk = 1024;
 constexpr int kSlotPerLane = kSlotChunk / (kWarps * 32);  // slots per lane per chunk
 
 // Lane slots of a chunk starting at `begin` of the depth-sorted slots, and
-// their tile-row ranges (empty for a culled slot).
+// their tile-row ranges and (with xr) tile-column ranges, empty for a culled
+// slot. A culled slot is known by its sorted key (kCulledKey, read beside the
+// slot), so the only gather by slot is its rectangle; a visible slot's
+// rectangle is never empty (its footprint meets the image).
 __device__ __forceinline__ void chunk_slot_rows(const uint32_t* __restrict__ sorted_slots,
-                                                const int32_t* __restrict__ tile_count,
+                                                const uint32_t* __restrict__ sorted_keys,
                                                 const uint2* __restrict__ rect, int64_t begin,
                                                 uint32_t (&slot)[kSlotPerLane],
-                                                uint32_t (&yr)[kSlotPerLane]) {
+                                                uint32_t (&yr)[kSlotPerLane],
+                                                uint32_t (*xr)[kSlotPerLane] = nullptr) {
   const int w = warp_id(), lane = lane_id();
+  bool live[kSlotPerLane];
 #pragma unroll
   for (int k = 0; k < kSlotPerLane; ++k) {
     const int64_t i = begin + w * (kSlotChunk / kWarps) + k * 32 + lane;
     slot[k] = sorted_slots[i];
+    live[k] = sorted_keys[i] != kCulledKey;
     yr[k] = 1u;  // y0 = 1 > y1 = 0: no rows
+    if (xr != nullptr) (*xr)[k] = 1u;
   }
 #pragma unroll
   for (int k = 0; k < kSlotPerLane; ++k)
-    if (tile_count[slot[k]] > 0) yr[k] = rect[slot[k]].y;
+    if (live[k]) {
+      const uint2 r = rect[slot[k]];
+      yr[k] = r.y;
+      if (xr != nullptr) (*xr)[k] = r.x;
+    }
 }
 
 // counts[(row_offset + y) * cpv + c]: splats of chunk c of view v (block
 // v * cpv + c) covering tile row y of the view.
 __global__ void __launch_bounds__(kWarps * 32)
     k_slot_row_counts(const uint32_t* __restrict__ sorted_slots,
-                      const int32_t* __restrict__ tile_count, const uint2* __restrict__ rect,
+                      const uint32_t* __restrict__ sorted_keys, const uint2* __restrict__ rect,
                       const ViewDesc* __restrict__ views, int64_t slot_stride, int cpv,
                       int max_tiles_y, int32_t* __restrict__ counts) {
   extern __shared__ int32_t s_cnt[];  // [kWarps][max_tiles_y]
@@ -478,8 +489,8 @@ __global__ void __launch_bounds__(kWarps * 32)
     s_cnt[(i / tiles_y) * max_tiles_y + (i % tiles_y)] = 0;
   __syncthreads();
   uint32_t slot[kSlotPerLane], yr[kSlotPerLane];
-  chunk_slot_rows(sorted_slots, tile_count, rect, (int64_t)v * slot_stride + (int64_t)c * kSlotChunk,
-                  slot, yr);
+  chunk_slot_rows(sorted_slots, sorted_keys, rect,
+                  (int64_t)v * slot_stride + (int64_t)c * kSlotChunk, slot, yr);
   warp_range_counts(yr, tiles_y, s_cnt + warp_id() * max_tiles_y);
   __syncthreads();
   for (int y = threadIdx.x; y < tiles_y; y += blockDim.x) {
@@ -494,7 +505,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 // row y, in slot order; nothing at or past `capacity`.
 __global__ void __launch_bounds__(kWarps * 32)
     k_slot_row_expand(const uint32_t* __restrict__ sorted_slots,
-                      const int32_t* __restrict__ tile_count, const uint2* __restrict__ rect,
+                      const uint32_t* __restrict__ sorted_keys, const uint2* __restrict__ rect,
                       const ViewDesc* __restrict__ views, int64_t slot_stride, int cpv,
                       int max_tiles_y, const int64_t* __restrict__ offsets, int64_t capacity,
                       uint32_t* __restrict__ rec_slots, uint32_t* __restrict__ rec_xr) {
@@ -511,18 +522,14 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   __syncthreads();
   uint32_t slot[kSlotPerLane], yr[kSlotPerLane];
-  chunk_slot_rows(sorted_slots, tile_count, rect, (int64_t)v * slot_stride + (int64_t)c * kSlotChunk,
-                  slot, yr);
+  uint32_t xr[kSlotPerLane];  // the column ranges, written beside the records
+  chunk_slot_rows(sorted_slots, sorted_keys, rect,
+                  (int64_t)v * slot_stride + (int64_t)c * kSlotChunk, slot, yr, &xr);
   warp_range_counts(yr, tiles_y, e.cnt + w * max_tiles_y);
   __syncthreads();
   const bool staged = chunk_layout(
       e.cnt, max_tiles_y, tiles_y, kStage, s_warp, e.col_count, e.col_start, e.col_dst,
       [&](int y) { return offsets[(int64_t)(vd.row_offset + y) * cpv + c]; });
-  uint32_t xr[kSlotPerLane];  // the column ranges, written beside the records
-  if (!staged) {
-#pragma unroll
-    for (int k = 0; k < kSlotPerLane; ++k) xr[k] = rect[slot[k]].x;
-  }
   warp_range_expand(yr, slot, e.cnt + w * max_tiles_y, e.bitmap + w * max_tiles_y, staged,
                     e.stage, e.col_start, e.col_dst, capacity, rec_slots, &xr, rec_xr);
   if (!staged) return;
@@ -570,7 +577,7 @@ void configure_bin_kernels() {
 
 int slot_chunks_per_view(int64_t slot_stride) { return (int)(slot_stride / kSlotChunk); }
 
-void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
+void launch_slot_row_counts(const uint32_t* sorted_slots, const uint32_t* sorted_keys,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, int32_t* counts,
                             cudaStream_t stream) {
@@ -578,11 +585,11 @@ void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_co
   if (n_views <= 0 || cpv <= 0) return;
   count_launch();
   k_slot_row_counts<<<(unsigned)(n_views * cpv), kWarps * 32, slot_row_counts_smem(max_tiles_y),
-                      stream>>>(sorted_slots, tile_count, rect, views, slot_stride, cpv,
+                      stream>>>(sorted_slots, sorted_keys, rect, views, slot_stride, cpv,
                                 max_tiles_y, counts);
 }
 
-void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
+void launch_slot_row_expand(const uint32_t* sorted_slots, const uint32_t* sorted_keys,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
                             int64_t capacity, uint32_t* rec_slots, uint32_t* rec_xr,
@@ -591,7 +598,7 @@ void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_co
   if (n_views <= 0 || cpv <= 0) return;
   count_launch();
   k_slot_row_expand<<<(unsigned)(n_views * cpv), kWarps * 32, chunk_expand_smem(max_tiles_y),
-                      stream>>>(sorted_slots, tile_count, rect, views, slot_stride, cpv,
+                      stream>>>(sorted_slots, sorted_keys, rect, views, slot_stride, cpv,
                                 max_tiles_y, offsets, capacity, rec_slots, rec_xr);
 }
 

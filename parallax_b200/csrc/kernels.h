@@ -65,11 +65,11 @@ void configure_bin_kernels();  // once per device, outside graph capture
 // view, counts[(row_offset + y) * cpv + c]; after their exclusive scan into
 // offsets, each chunk writes its records (slot ids) at its bases.
 int slot_chunks_per_view(int64_t slot_stride);
-void launch_slot_row_counts(const uint32_t* sorted_slots, const int32_t* tile_count,
+void launch_slot_row_counts(const uint32_t* sorted_slots, const uint32_t* sorted_keys,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, int32_t* counts,
                             cudaStream_t stream);
-void launch_slot_row_expand(const uint32_t* sorted_slots, const int32_t* tile_count,
+void launch_slot_row_expand(const uint32_t* sorted_slots, const uint32_t* sorted_keys,
                             const uint2* rect, const ViewDesc* views, int n_views,
                             int64_t slot_stride, int max_tiles_y, const int64_t* offsets,
                             int64_t capacity, uint32_t* rec_slots, uint32_t* rec_xr,

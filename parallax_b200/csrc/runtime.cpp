@@ -232,13 +232,13 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
   uint32_t *ka = sort_keys_alt.get(), *va = sort_vals_alt.get();
   radix_sort_pairs(k, v, ka, va, slots, slot_stride, 32, hist.get(), hist_scanned.get(), scan_,
                    stream);
-  sorted_slots = v;
+  sorted_slots = v;  // k holds their keys: kCulledKey for a culled slot
   // 2. one record per covered tile row, grouped by row and near to far within
   //    a row: per (view, slot chunk) row counts, their scan in (row, chunk)
   //    order, then each chunk writes its records at its bases
   const int cpv = slot_chunks_per_view(slot_stride);
   const int64_t n_row_chunks = static_cast<int64_t>(batch.total_rows) * cpv;
-  launch_slot_row_counts(v, tile_count.get(), rect.get(), d_views.get(), V, slot_stride,
+  launch_slot_row_counts(v, k, rect.get(), d_views.get(), V, slot_stride,
                          batch.max_tiles_y, row_chunk_counts.get(), stream);
   exclusive_scan_i32_to_i64(row_chunk_counts.get(), row_chunk_offsets.get(), n_row_chunks,
                             d_total_records.get(), scan_, stream);
@@ -253,7 +253,7 @@ int64_t Frame::bin(bool host_sync, cudaStream_t stream) {
     throw Error(PXS_ERR_INVALID, "pair buffers must be reserved before an unsynchronised bin");
   }
   PXS_CUDA(cudaMemsetAsync(overflow.get(), 0, sizeof(int32_t), stream));
-  launch_slot_row_expand(v, tile_count.get(), rect.get(), d_views.get(), V, slot_stride,
+  launch_slot_row_expand(v, k, rect.get(), d_views.get(), V, slot_stride,
                          batch.max_tiles_y, row_chunk_offsets.get(), record_capacity,
                          rec_vals.get(), rec_xr.get(), stream);
   launch_row_ranges_from_chunks(row_chunk_offsets.get(), batch.total_rows, cpv,
