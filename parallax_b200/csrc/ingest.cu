@@ -7,6 +7,8 @@
 // edges from 64-bit products, the sum rounded by adding half the count) and
 // writes the byte and / or the float; the 8-bit frame crosses PCIe instead of
 // the four times larger float image.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -67,6 +69,55 @@ __global__ void __launch_bounds__(256)
   const uint8_t b = src[i];
   if (out_bytes != nullptr) out_bytes[i] = b;
   if (out_linear != nullptr) out_linear[i] = (float)b / 255.f;
+}
+
+// Several frames already at their view's size in one launch: thread i
+// converts 16-byte group i of the frames laid end to end (frame j holds
+// groups [start[j], start[j + 1])), with the arithmetic of k_bytes_to_linear16.
+struct LinearFrames {
+  const uint4* src[kMaxLinearFrames];
+  float4* out[kMaxLinearFrames];
+  int64_t start[kMaxLinearFrames + 1];
+  int count;
+};
+
+__global__ void __launch_bounds__(256) k_bytes_to_linear16_frames(LinearFrames f) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= f.start[f.count]) return;
+  int j = 0;
+  while (j + 1 < f.count && f.start[j + 1] <= i) ++j;
+  const int64_t g = i - f.start[j];
+  const uint4 w = f.src[j][g];
+  const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t v = words[k];
+    f.out[j][g * 4 + k] = make_float4((float)(v & 0xFFu) / 255.f, (float)((v >> 8) & 0xFFu) / 255.f,
+                                      (float)((v >> 16) & 0xFFu) / 255.f, (float)(v >> 24) / 255.f);
+  }
+}
+
+bool linear_frame_ok(const uint8_t* src, const float* out, int64_t bytes) {
+  return bytes > 0 && bytes % 16 == 0 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0 &&
+         (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
+}
+
+void launch_bytes_to_linear_frames(const uint8_t* const* src, float* const* out,
+                                   const int64_t* bytes, int n, cudaStream_t stream) {
+  for (int first = 0; first < n; first += kMaxLinearFrames) {
+    LinearFrames f;
+    f.count = std::min(kMaxLinearFrames, n - first);
+    f.start[0] = 0;
+    for (int j = 0; j < f.count; ++j) {
+      f.src[j] = reinterpret_cast<const uint4*>(src[first + j]);
+      f.out[j] = reinterpret_cast<float4*>(out[first + j]);
+      f.start[j + 1] = f.start[j] + bytes[first + j] / 16;
+    }
+    const int64_t groups = f.start[f.count];
+    if (groups <= 0) continue;
+    count_launch();
+    k_bytes_to_linear16_frames<<<(unsigned)((groups + 255) / 256), 256, 0, stream>>>(f);
+  }
 }
 
 void launch_downscale(const uint8_t* src, int width, int height, int out_width, int out_height,

@@ -170,6 +170,14 @@ void launch_seed_points(const float* points, const uint8_t* colors, int n, int S
 // ingest.cu: downscaleToWidth's box filter (and the /255 to float) on the device
 void launch_downscale(const uint8_t* src, int width, int height, int out_width, int out_height,
                       uint8_t* out_bytes, float* out_linear, cudaStream_t stream);
+// Frames already at their view's size, bytes to linear floats (byte / 255,
+// as launch_downscale writes for them), up to kMaxLinearFrames per launch.
+// Each frame must pass linear_frame_ok: a whole number of 16-byte groups,
+// both addresses 16-byte aligned.
+constexpr int kMaxLinearFrames = 16;
+bool linear_frame_ok(const uint8_t* src, const float* out, int64_t bytes);
+void launch_bytes_to_linear_frames(const uint8_t* const* src, float* const* out,
+                                   const int64_t* bytes, int n, cudaStream_t stream);
 
 // peak.cu
 float measure_fp32_peak_tflops(cudaStream_t stream);

@@ -323,11 +323,29 @@ struct pxs_trainer {
       const StagedSet& set = pending[i];
       const int k = set.slot;
       PXS_CUDA(cudaStreamWaitEvent(stream, staged_event[k], 0));
+      // frames at their view's size go through one launch for the set; the
+      // others are downscaled one by one
+      std::vector<const uint8_t*> src;
+      std::vector<float*> dst;
+      std::vector<int64_t> bytes;
       for (const StagedFrame& f : set.frames) {
-        pxs::launch_downscale(stage_buf[k].get() + f.offset, f.width, f.height, f.out_width,
-                              f.out_height, nullptr,
-                              images.get() + image_offset[static_cast<size_t>(f.view)] * 3,
+        const uint8_t* in = stage_buf[k].get() + f.offset;
+        float* out = images.get() + image_offset[static_cast<size_t>(f.view)] * 3;
+        const int64_t n = static_cast<int64_t>(f.width) * f.height * 3;
+        if (f.width == f.out_width && f.height == f.out_height &&
+            pxs::linear_frame_ok(in, out, n)) {
+          src.push_back(in);
+          dst.push_back(out);
+          bytes.push_back(n);
+          continue;
+        }
+        pxs::launch_downscale(in, f.width, f.height, f.out_width, f.out_height, nullptr, out,
                               stream);
+        PXS_CUDA(cudaGetLastError());
+      }
+      if (!src.empty()) {
+        pxs::launch_bytes_to_linear_frames(src.data(), dst.data(), bytes.data(),
+                                           static_cast<int>(src.size()), stream);
         PXS_CUDA(cudaGetLastError());
       }
       PXS_CUDA(cudaEventRecord(consumed_event[k], stream));

@@ -93,30 +93,33 @@ def test_seed_matches_the_reference(n, sh, with_colors):
 
 
 @pytest.mark.gpu
-def test_staged_frames_train_like_ingested_frames():
+@pytest.mark.parametrize("fw,fh", [(640, 480), (160, 120)])
+def test_staged_frames_train_like_ingested_frames(fw, fh):
     """pxs_trainer_stage_images, pipelined the way a feeding loop uses it (the
     next step's frames staged before the current step runs), takes the same
     steps as ingesting each step's frames synchronously: same losses and the
-    same cloud up to the order of the adjoint's atomic sums."""
+    same cloud up to the order of the adjoint's atomic sums. Frames four times
+    the view's width are downscaled one by one; frames at the view's size are
+    converted together, one launch per staged set."""
     params, rest = O.random_cloud(72, 3000, 1)
     cloud = px.GaussianCloud(params, 1, rest)
     views = O.orbit_views(6, 160, 120, seed=4)
     blank = np.zeros(160 * 120 * 3, np.float32)
     rs = np.random.default_rng(9)
-    frames = [rs.integers(0, 256, 640 * 480 * 3, dtype=np.uint8) for _ in range(6)]
+    frames = [rs.integers(0, 256, fw * fh * 3, dtype=np.uint8) for _ in range(6)]
     schedule = [[0, 1], [2, 3], [4, 5], [1, 4], [3, 0]]
     cfg = px.TrainConfig(iterations=50, sh_degree=1, sh_increase_interval=0)
     sync = px.SplatTrainer(cloud, [(v.camera(), blank) for v in views], cfg)
     staged = px.SplatTrainer(cloud, [(v.camera(), blank) for v in views], cfg)
     losses_sync, losses_staged = [], []
     for ids in schedule:
-        sync.ingest_images(ids, [frames[i] for i in ids], [(640, 480)] * len(ids))
+        sync.ingest_images(ids, [frames[i] for i in ids], [(fw, fh)] * len(ids))
         losses_sync.append(sync.step_batch(len(ids), ids))
-    staged.stage_images(schedule[0], [frames[i] for i in schedule[0]], [(640, 480)] * 2)
+    staged.stage_images(schedule[0], [frames[i] for i in schedule[0]], [(fw, fh)] * 2)
     for s, ids in enumerate(schedule):
         if s + 1 < len(schedule):
             nxt = schedule[s + 1]
-            staged.stage_images(nxt, [frames[i] for i in nxt], [(640, 480)] * len(nxt))
+            staged.stage_images(nxt, [frames[i] for i in nxt], [(fw, fh)] * len(nxt))
         losses_staged.append(staged.step_batch(len(ids), ids))
     assert np.allclose(losses_sync, losses_staged, rtol=1e-6, atol=0)
     # the adjoint sums with atomics in no fixed order: clouds agree to rounding
