@@ -6,8 +6,9 @@
 // stops as soon as every pixel has reached the transmittance cutoff
 // (__syncthreads_and). Arithmetic follows rasterizeSplats
 // (SplatRaster.cpp:285-310) term for term, rounded the same way (the file is
-// compiled with -fmad=false); exp is CUDA's expf, skipped only where the
-// alpha floor certainly rejects the pair (power_floor).
+// compiled with -fmad=false); exp is splat_exp (the hardware exponential,
+// raster_common.cuh), skipped only where the alpha floor certainly rejects the
+// pair (power_floor).
 #include <algorithm>
 
 #include "common.cuh"
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
             const float dy = fy[p] - m.y;
             const float power = splat_power(co, dx, dy);
             if (!(power > 0.f || power < floor)) {
-              float alpha = co.w * expf(power);
+              float alpha = co.w * splat_exp(power);
               alpha = alpha < kMaxAlpha ? alpha : kMaxAlpha;
               if (!(alpha < min_alpha)) {
                 if (kCount) ++contributing;
@@ -228,8 +229,8 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       // No early return for an entry that misses both pixels: a pixel that
       // does not take the entry adds T * 0 to its colour and keeps T, so the
       // body runs branch-free across the warp (measured 2.8% faster at C4).
-      float a0 = in0 ? co.w * expf(power.x) : 0.f;
-      float a1 = in1 ? co.w * expf(power.y) : 0.f;
+      float a0 = in0 ? co.w * splat_exp(power.x) : 0.f;
+      float a1 = in1 ? co.w * splat_exp(power.y) : 0.f;
       a0 = a0 < kMaxAlpha ? a0 : kMaxAlpha;
       a1 = a1 < kMaxAlpha ? a1 : kMaxAlpha;
       const bool c0 = in0 && !(a0 < min_alpha);

@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
           const float dy = fy[p] - m.y;
           const float power = splat_power(co, dx, dy);
           if (!(power > 0.f) && !(power < c.w)) {
-            const float gw = expf(power);
+            const float gw = splat_exp(power);
             const float raw_alpha = __fmul_rn(co.w, gw);
             const float alpha = raw_alpha < kMaxAlpha ? raw_alpha : kMaxAlpha;
             if (!(alpha < min_alpha)) {
@@ -391,8 +391,8 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         const float2 power = splat_power2(co, dx, dy);
         const bool in0 = e < last0[q] && !(power.x > 0.f) && !(power.x < c.w);
         const bool in1 = e < last1[q] && !(power.y > 0.f) && !(power.y < c.w);
-        const float g0 = in0 ? expf(power.x) : 0.f;
-        const float g1 = in1 ? expf(power.y) : 0.f;
+        const float g0 = in0 ? splat_exp(power.x) : 0.f;
+        const float g1 = in1 ? splat_exp(power.y) : 0.f;
         const float r0 = __fmul_rn(co.w, g0), r1 = __fmul_rn(co.w, g1);
         const float a0 = r0 < kMaxAlpha ? r0 : kMaxAlpha;
         const float a1 = r1 < kMaxAlpha ? r1 : kMaxAlpha;
