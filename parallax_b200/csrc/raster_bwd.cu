@@ -391,8 +391,11 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         const float2 power = splat_power2(co, dx, dy);
         const bool in0 = e < last0[q] && !(power.x > 0.f) && !(power.x < c.w);
         const bool in1 = e < last1[q] && !(power.y > 0.f) && !(power.y < c.w);
-        const float g0 = in0 ? splat_exp(power.x) : 0.f;
-        const float g1 = in1 ? splat_exp(power.y) : 0.f;
+        // not zeroed outside in0 / in1: every gradient term carries g through
+        // z or dLw, which are 0 there, and g is finite (a conic of a positive
+        // definite covariance gives power <= 0, so g <= 1)
+        const float g0 = splat_exp(power.x);
+        const float g1 = splat_exp(power.y);
         const float r0 = __fmul_rn(co.w, g0), r1 = __fmul_rn(co.w, g1);
         const float a0 = r0 < kMaxAlpha ? r0 : kMaxAlpha;
         const float a1 = r1 < kMaxAlpha ? r1 : kMaxAlpha;
