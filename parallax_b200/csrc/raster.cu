@@ -244,16 +244,14 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
       acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
       acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
-      if (c0) {
-        T.x *= 1.f - a0;
-        last0 = base + j + 1;
-        if (T.x < cutoff) done0 = true;
-      }
-      if (c1) {
-        T.y *= 1.f - a1;
-        last1 = base + j + 1;
-        if (T.y < cutoff) done1 = true;
-      }
+      // the products for both pixels, kept where the pixel takes the entry
+      const float t0 = T.x * (1.f - a0), t1 = T.y * (1.f - a1);
+      T.x = c0 ? t0 : T.x;
+      T.y = c1 ? t1 : T.y;
+      last0 = c0 ? base + j + 1 : last0;
+      last1 = c1 ? base + j + 1 : last1;
+      done0 = done0 || (c0 && t0 < cutoff);
+      done1 = done1 || (c1 && t1 < cutoff);
       return done0 && done1;
     };
     if (kCount) {

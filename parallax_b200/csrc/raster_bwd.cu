@@ -403,8 +403,10 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         const bool c1 = in1 && !(a1 < min_alpha);
         contrib = contrib || c0 || c1;
         const float2 alpha = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
-        const float2 inv = make_float2(c0 ? __fdividef(1.f, 1.f - alpha.x) : 1.f,
-                                       c1 ? __fdividef(1.f, 1.f - alpha.y) : 1.f);
+        // the reciprocals for both pixels, then 1 where the pixel does not
+        // take the entry (its T stays as it is)
+        const float q0 = __fdividef(1.f, 1.f - alpha.x), q1 = __fdividef(1.f, 1.f - alpha.y);
+        const float2 inv = make_float2(c0 ? q0 : 1.f, c1 ? q1 : 1.f);
         T[q] = __fmul2_rn(T[q], inv);
         const float2 weight = __fmul2_rn(alpha, T[q]);
         const float2 w6 = __fmul2_rn(weight, dLp0[q]);
