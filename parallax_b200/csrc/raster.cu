@@ -240,18 +240,22 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
       if (kBits && (c0 || c1)) s_took[warp][j] = 1;  // same value from every lane
       const float4 c = s_col[j];
-      const float2 ta = make_float2(c0 ? T.x * a0 : 0.f, c1 ? T.y * a1 : 0.f);
+      // alpha where the pixel takes the entry, else 0: the colour weight is
+      // then T * 0 = 0 and T * (1 - 0) = T is exact, so T needs no select
+      const float ac0 = c0 ? a0 : 0.f, ac1 = c1 ? a1 : 0.f;
+      const float2 ta = make_float2(T.x * ac0, T.y * ac1);
       acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
       acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
       acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
-      // the products for both pixels, kept where the pixel takes the entry
-      const float t0 = T.x * (1.f - a0), t1 = T.y * (1.f - a1);
-      T.x = c0 ? t0 : T.x;
-      T.y = c1 ? t1 : T.y;
+      const float t0 = T.x * (1.f - ac0), t1 = T.y * (1.f - ac1);
+      T.x = t0;
+      T.y = t1;
       last0 = c0 ? base + j + 1 : last0;
       last1 = c1 ? base + j + 1 : last1;
-      done0 = done0 || (c0 && t0 < cutoff);
-      done1 = done1 || (c1 && t1 < cutoff);
+      // T changes only where the pixel takes the entry, and a pixel is done
+      // once its T is below the cutoff, so no test of c0 / c1 is needed
+      done0 = done0 || t0 < cutoff;
+      done1 = done1 || t1 < cutoff;
       return done0 && done1;
     };
     if (kCount) {
