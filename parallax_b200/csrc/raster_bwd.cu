@@ -389,8 +389,10 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
       for (int q = 0; q < NP; ++q) {
         const float2 dy = make_float2(fy[q].x - m.y, fy[q].y - m.y);
         const float2 power = splat_power2(co, dx, dy);
-        const bool in0 = e < last0[q] && !(power.x > 0.f) && !(power.x < c.w);
-        const bool in1 = e < last1[q] && !(power.y > 0.f) && !(power.y < c.w);
+        // no power-floor test: below the floor alpha is certainly under
+        // min_alpha, so the alpha test below decides the same
+        const bool in0 = e < last0[q] && !(power.x > 0.f);
+        const bool in1 = e < last1[q] && !(power.y > 0.f);
         // not zeroed outside in0 / in1: every gradient term carries g through
         // z or dLw, which are 0 there, and g is finite (a conic of a positive
         // definite covariance gives power <= 0, so g <= 1)
