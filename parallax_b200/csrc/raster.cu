@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
 }
 
 // The two-pixel form of k_forward: each thread composites two vertically
-// adjacent pixels of one column. Power, alpha and transmittance are the
+// adjacent pixels of one column. Power, alpha and transmittance round as the
 // scalar operations of k_forward (so the same entries are taken and T is
 // bit-identical); the colour sums of the two pixels are one paired fused
 // multiply-add per channel (fma.rn.f32x2), which differs from the separate
@@ -163,9 +163,9 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
                  uint8_t* __restrict__ block_bits, int schedule, const int* __restrict__ order,
                  int* __restrict__ ticket, int total_tiles) {
   constexpr int kThreads = TileGeom<2>::kThreads;
-  __shared__ float2 s_xy[kFwdBatch];
-  __shared__ float4 s_co[kFwdBatch];
-  __shared__ float4 s_col[kFwdBatch];  // r, g, b, power floor
+  __shared__ float2 s_xy[kFwdBatch];  // -mean
+  __shared__ float4 s_co[kFwdBatch];  // conic, -opacity
+  __shared__ float4 s_col[kFwdBatch];  // -r, -g, -b, 0
   __shared__ uint32_t s_mask[kFwdBatch];
   __shared__ uint8_t s_took[TileGeom<2>::kWarps][kFwdBatch];  // warp w = 8x8 block w
   __shared__ uint8_t s_list[TileGeom<2>::kWarps][kFwdBatch];  // a warp's entries of the batch
@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
   const int warp = threadIdx.x >> 5;
   const ViewDesc& vd = views[info.view];
   const float min_alpha = vd.min_alpha, cutoff = vd.transmittance_cutoff;
+  const float neg_min_alpha = -min_alpha;
   const float fx = (float)info.px + 0.5f;
   const float2 fy = make_float2((float)info.py0 + 0.5f, (float)(info.py0 + 1) + 0.5f);
   const bool col_in = info.px < vd.cam.width;
@@ -208,20 +209,27 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       const uint32_t slot = pair_slots[base + i];
       const float4 co = conic_op[slot];
       const float2 mean = xy[slot];
-      float4 c = color[slot];
-      c.w = power_floor(co.w, min_alpha);
-      s_xy[i] = mean;
-      s_co[i] = co;
-      s_col[i] = c;
-      s_mask[i] = warp_mask<2, true>(mean, co, c.w, info.tile_px, info.tile_py);
+      const float4 c = color[slot];
+      // staged negated (see visit): the mean, the opacity and the colour
+      s_xy[i] = make_float2(-mean.x, -mean.y);
+      s_co[i] = make_float4(co.x, co.y, co.z, -co.w);
+      s_col[i] = make_float4(-c.x, -c.y, -c.z, 0.f);
+      s_mask[i] = warp_mask<2, true>(mean, co, power_floor(co.w, min_alpha), info.tile_px,
+                                     info.tile_py);
     }
     __syncthreads();
-    // entry j for this warp's pixels; returns whether both are done
+    // entry j for this warp's pixels; returns whether both are done. The two
+    // pixels' operations run as paired f32x2 instructions with the scalar
+    // roundings (mul2_rn, add2_rn). The mean, opacity and colour are staged
+    // negated, and each negation is exact and undone exactly: fx + (-mx) is
+    // fx - mx; (-o) e is -(o e), so alpha's tests and cap are mirrored;
+    // (-T alpha)(-r) is (T alpha) r in the colour FMA; 1 + (-alpha) is
+    // 1 - alpha.
     auto visit = [&](int j) -> bool {
-      const float2 m = s_xy[j];
+      const float2 nm = s_xy[j];
       const float4 co = s_co[j];
-      const float dx = fx - m.x;
-      const float2 dy = make_float2(fy.x - m.y, fy.y - m.y);
+      const float dx = fx + nm.x;
+      const float2 dy = add2_rn(fy, make_float2(nm.y, nm.y));
       const float2 power = splat_power2(co, dx, dy);
       // (the power floor only spares the exp elsewhere: below it alpha is
       // certainly under min_alpha, so the alpha test decides the same)
@@ -230,33 +238,31 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       // No early return for an entry that misses both pixels: a pixel that
       // does not take the entry adds T * 0 to its colour and keeps T, so the
       // body runs branch-free across the warp (measured 2.8% faster at C4).
-      // alpha is read only where c0 / c1 (which include in0 / in1) hold, so
+      // -alpha, read only where c0 / c1 (which include in0 / in1) hold, so
       // it needs no zeroing outside them
-      float a0 = co.w * splat_exp(power.x);
-      float a1 = co.w * splat_exp(power.y);
-      a0 = a0 < kMaxAlpha ? a0 : kMaxAlpha;
-      a1 = a1 < kMaxAlpha ? a1 : kMaxAlpha;
-      const bool c0 = in0 && !(a0 < min_alpha);
-      const bool c1 = in1 && !(a1 < min_alpha);
+      float2 na = mul2_rn(make_float2(co.w, co.w),
+                          make_float2(splat_exp(power.x), splat_exp(power.y)));
+      na.x = na.x > -kMaxAlpha ? na.x : -kMaxAlpha;
+      na.y = na.y > -kMaxAlpha ? na.y : -kMaxAlpha;
+      const bool c0 = in0 && !(na.x > neg_min_alpha);
+      const bool c1 = in1 && !(na.y > neg_min_alpha);
       if (kCount) contributing += (c0 ? 1 : 0) + (c1 ? 1 : 0);
       if (kBits && (c0 || c1)) s_took[warp][j] = 1;  // same value from every lane
-      const float4 c = s_col[j];
-      // alpha where the pixel takes the entry, else 0: the colour weight is
-      // then T * 0 = 0 and T * (1 - 0) = T is exact, so T needs no select
-      const float ac0 = c0 ? a0 : 0.f, ac1 = c1 ? a1 : 0.f;
-      const float2 ta = make_float2(T.x * ac0, T.y * ac1);
-      acc0 = __ffma2_rn(ta, make_float2(c.x, c.x), acc0);
-      acc1 = __ffma2_rn(ta, make_float2(c.y, c.y), acc1);
-      acc2 = __ffma2_rn(ta, make_float2(c.z, c.z), acc2);
-      const float t0 = T.x * (1.f - ac0), t1 = T.y * (1.f - ac1);
-      T.x = t0;
-      T.y = t1;
+      const float4 nc = s_col[j];
+      // -alpha where the pixel takes the entry, else 0: the colour weight is
+      // then T * 0 = 0 and T * (1 + 0) = T is exact, so T needs no select
+      const float2 nac = make_float2(c0 ? na.x : 0.f, c1 ? na.y : 0.f);
+      const float2 nta = mul2_rn(T, nac);
+      acc0 = __ffma2_rn(nta, make_float2(nc.x, nc.x), acc0);
+      acc1 = __ffma2_rn(nta, make_float2(nc.y, nc.y), acc1);
+      acc2 = __ffma2_rn(nta, make_float2(nc.z, nc.z), acc2);
+      T = mul2_rn(T, add2_rn(make_float2(1.f, 1.f), nac));
       last0 = c0 ? base + j + 1 : last0;
       last1 = c1 ? base + j + 1 : last1;
       // T changes only where the pixel takes the entry, and a pixel is done
       // once its T is below the cutoff, so no test of c0 / c1 is needed
-      done0 = done0 || t0 < cutoff;
-      done1 = done1 || t1 < cutoff;
+      done0 = done0 || T.x < cutoff;
+      done1 = done1 || T.y < cutoff;
       return done0 && done1;
     };
     if (kCount) {

@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
   __shared__ uint32_t s_slot[kB];
   __shared__ float2 s_xy[kB];
   __shared__ float4 s_co[kB];
-  __shared__ float4 s_col[kB];  // r, g, b, power floor
+  __shared__ float4 s_col[kB];  // r, g, b (w unused)
   __shared__ uint32_t s_mask[kB];
   __shared__ float s_acc[kB][12];
   __shared__ uint8_t s_list[kWarps][kB];  // a warp's entries of the batch
@@ -342,17 +342,16 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
       const uint32_t slot = pair_slots[batch_start + i];
       const float4 co = conic_op[slot];
       const float2 mean = xy[slot];
-      float4 c = color[slot];
-      c.w = power_floor(co.w, min_alpha);
       s_slot[i] = slot;
-      s_xy[i] = mean;
+      s_xy[i] = make_float2(-mean.x, -mean.y);  // negated: fx + (-mx) is fx - mx
       s_co[i] = co;
-      s_col[i] = c;
+      s_col[i] = color[slot];
       // which warps took the entry in the forward pass (exact), else which
       // ones its footprint can reach
       s_mask[i] = block_bits != nullptr
                       ? mask_from_block_bits<PX>(block_bits[batch_start + i])
-                      : warp_mask<PX>(mean, co, c.w, info.tile_px, info.tile_py);
+                      : warp_mask<PX>(mean, co, power_floor(co.w, min_alpha), info.tile_px,
+                                      info.tile_py);
 #pragma unroll
       for (int k = 0; k < 12; ++k) s_acc[i][k] = 0.f;
     }
@@ -372,10 +371,10 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
     for (int qi = n_mine - 1; qi >= 0; --qi) {  // back to front
       const int j = s_list[warp][qi];
       const int e = batch_start + j;
-      const float2 m = s_xy[j];
+      const float2 nm = s_xy[j];
       const float4 co = s_co[j];
       const float4 c = s_col[j];
-      const float dx = fx - m.x;
+      const float dx = fx + nm.x;
       bool contrib = false, touched = false;
       float v[10];
 #pragma unroll
@@ -387,7 +386,7 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
       };
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
-        const float2 dy = make_float2(fy[q].x - m.y, fy[q].y - m.y);
+        const float2 dy = add2_rn(fy[q], make_float2(nm.y, nm.y));
         const float2 power = splat_power2(co, dx, dy);
         // no power-floor test: below the floor alpha is certainly under
         // min_alpha, so the alpha test below decides the same
@@ -398,7 +397,8 @@ __global__ void __launch_bounds__(TileGeom<2 * NP>::kThreads)
         // definite covariance gives power <= 0, so g <= 1)
         const float g0 = splat_exp(power.x);
         const float g1 = splat_exp(power.y);
-        const float r0 = __fmul_rn(co.w, g0), r1 = __fmul_rn(co.w, g1);
+        const float2 r = mul2_rn(make_float2(co.w, co.w), make_float2(g0, g1));
+        const float r0 = r.x, r1 = r.y;
         const float a0 = r0 < kMaxAlpha ? r0 : kMaxAlpha;
         const float a1 = r1 < kMaxAlpha ? r1 : kMaxAlpha;
         const bool c0 = in0 && !(a0 < min_alpha);

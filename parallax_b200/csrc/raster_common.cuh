@@ -103,6 +103,42 @@ __device__ __forceinline__ void for_each_tile(int schedule, const int* __restric
   }
 }
 
+// Paired FP32 multiply, add and fused multiply-add (f32x2) as inline PTX
+// with round-to-nearest. Each component rounds as the scalar __fmul_rn /
+// __fadd_rn / __fmaf_rn does (checked against them on random pairs). A paired
+// add whose operand is a paired product was nevertheless found contracted
+// into one rounding in the generated code, so the exact paths never feed a
+// paired product straight into a paired add (splat_power2); the compositing
+// tests hold the two-pixel kernels' transmittance bit-identical to the
+// one-pixel kernel's scalar arithmetic.
+__device__ __forceinline__ unsigned long long f2_to_b64(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 b64_to_f2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_to_b64(a)), "l"(f2_to_b64(b)));
+  return b64_to_f2(d);
+}
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_to_b64(a)), "l"(f2_to_b64(b)));
+  return b64_to_f2(d);
+}
+
+__device__ __forceinline__ float2 fma2_rn(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(d) : "l"(f2_to_b64(a)), "l"(f2_to_b64(b)), "l"(f2_to_b64(c)));
+  return b64_to_f2(d);
+}
+
 // The hardware square-root approximation (relative error about 2^-22).
 __device__ __forceinline__ float sqrt_approx(float x) {
   float r;
@@ -183,18 +219,26 @@ __device__ __forceinline__ float splat_power(const float4& co, float dx, float d
   return __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2)), t3);
 }
 
-// splat_power for the two pixels (dx, dy.x) and (dx, dy.y) of one column:
-// the same scalar operations, with the products that only involve dx shared.
-// (Paired f32x2 instructions are not used here: the code generator may fuse a
-// paired multiply and add into one rounding, and these values decide which
-// entries a pixel takes, so they must round exactly like the reference.)
+// splat_power for the two pixels (dx, dy.x) and (dx, dy.y) of one column,
+// with the reference's roundings:
+// - the products that only involve dx are shared scalars;
+// - the products (c dy) dy and (-b dx) dy are paired operations that round
+//   as the scalar ones (mul2_rn);
+// - a + b, with one operand a paired product, stays scalar: the code
+//   generator was found to contract a paired add fed by a paired product
+//   into one rounding;
+// - the last step, -0.5 (t1 + t2) - b dx dy, is one paired fused
+//   multiply-add. Halving is exact, so the fused product -0.5 s equals its
+//   rounded value (s >= 2^-125; a smaller nonzero s needs a conic entry
+//   below about 1e-24, a footprint of 1e12 pixels), and the addition of
+//   (-b dx) dy = -(b dx dy) equals the subtraction exactly, as rounding to
+//   nearest is symmetric.
 __device__ __forceinline__ float2 splat_power2(const float4& co, float dx, float2 dy) {
   const float t1 = __fmul_rn(__fmul_rn(co.x, dx), dx);
-  const float bdx = __fmul_rn(co.y, dx);
-  const float t2x = __fmul_rn(__fmul_rn(co.z, dy.x), dy.x);
-  const float t2y = __fmul_rn(__fmul_rn(co.z, dy.y), dy.y);
-  return make_float2(__fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2x)), __fmul_rn(bdx, dy.x)),
-                     __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(t1, t2y)), __fmul_rn(bdx, dy.y)));
+  const float nbdx = __fmul_rn(-co.y, dx);
+  const float2 t2 = mul2_rn(mul2_rn(make_float2(co.z, co.z), dy), dy);
+  const float2 s = make_float2(__fadd_rn(t1, t2.x), __fadd_rn(t1, t2.y));
+  return fma2_rn(make_float2(-0.5f, -0.5f), s, mul2_rn(make_float2(nbdx, nbdx), dy));
 }
 
 // exp(power) for alpha = opacity * exp(power) (SplatRaster.cpp:298), in
