@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
       }
       __syncwarp();
       if (!(done0 && done1))
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < n_mine; ++q)
           if (visit(s_list[warp][q])) break;
     }
