@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(TileGeom<PX>::kThreads)
 // or 256; 128 by default -- a tile stops at saturation, so a smaller batch
 // stages fewer entries past it); `schedule` maps CTAs to tiles (for_each_tile).
 template <bool kCount, bool kBits, int kFwdBatch>
-__global__ void __launch_bounds__(TileGeom<2>::kThreads, 10)
+__global__ void __launch_bounds__(TileGeom<2>::kThreads, 8)
     k_forward_x2(const int2* __restrict__ ranges, const uint32_t* __restrict__ pair_slots,
                  const float2* __restrict__ xy, const float4* __restrict__ conic_op,
                  const float4* __restrict__ color, const ViewDesc* __restrict__ views,

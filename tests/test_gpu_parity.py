@@ -347,6 +347,34 @@ def test_pixels_per_thread_variants_agree(ctx, fwd_px, bwd_px):
     assert lib.pxs_set_raster_config(3, 0) == px._abi.PXS_ERR_INVALID
 
 
+@pytest.mark.parametrize("seed,count,sh,size", [(5, 20000, 3, (640, 480)),
+                                                (6, 60000, 3, (333, 251)),
+                                                (7, 20000, 0, (480, 360))])
+def test_two_pixel_compositing_takes_the_one_pixel_kernels_entries(ctx, seed, count, sh, size):
+    """The two- and four-pixel compositing kernels round power, alpha and
+    transmittance as the one-pixel kernel's scalar operations (the two-pixel
+    form runs them as paired f32x2 instructions): on random clouds, dense
+    enough that most pixels saturate, transmittance is bit-identical and
+    colours agree to the paired colour FMA's rounding."""
+    lib = px.lib()
+    old_f, old_b = ct.c_int32(), ct.c_int32()
+    lib.pxs_get_raster_config(ct.byref(old_f), ct.byref(old_b))
+    view, opt, cloud = random_case(seed, count, sh, *size, log_scale_mean=-2.5)
+    out = {}
+    try:
+        for f in (1, 2, 4):
+            assert lib.pxs_set_raster_config(f, 2) == 0
+            out[f] = px.render_splats(cloud, view.camera(), opt, ctx)
+    finally:
+        lib.pxs_set_raster_config(old_f.value, old_b.value)
+    rgb1, T1 = out[1]
+    assert (T1 < 0.5).mean() > 0.2  # the lists are long enough to matter
+    for f in (2, 4):
+        rgb, T = out[f]
+        assert np.array_equal(T, T1), (f, int((T != T1).sum()))
+        assert np.abs(rgb - rgb1).max() <= 1e-5 * max(1.0, np.abs(rgb1).max())
+
+
 @pytest.mark.parametrize("shape", [(64, 256, 1, 1), (256, 64, 2, 2), (128, 128, 2, 1),
                                    (128, 256, 0, 2)])
 def test_batch_and_tile_schedule_leave_results_unchanged(ctx, shape):
