@@ -249,14 +249,15 @@ __device__ __forceinline__ uint32_t mask_from_block_bits(uint32_t bits) {
 // pixels per thread (NP = 1: two pixels, 8x8 blocks per warp; NP = 2: four
 // pixels, 8x16 blocks). The gradient arithmetic of a pair runs as the halves
 // of paired FP32 instructions (fma/add/mul .f32x2). The branch decisions are
-// the forward's, from the same scalar operations (splat_power2, alpha =
-// opacity * exp). The body has no branches on them: a pixel that does not
+// the forward's, from operations that round as its own (splat_power2, alpha
+// = opacity * exp). The body has no branches on them: a pixel that does not
 // take an entry runs the paired arithmetic with alpha = 0 and a zero loss
 // gradient, so its transmittance (multiplied by 1), its suffix colour (an FMA
 // with a zero weight) and its sums are unchanged; almost every warp has some
 // lane that takes the entry, so branching around the arithmetic only added
-// divergence handling (adjoint 8.87 -> 7.81 ms per C4 step). A thread adds its pairs' contributions before the warp
-// reduction, so one reduction serves 2 NP pixels per lane.
+// divergence handling (adjoint 8.87 -> 7.81 ms per C4 step). A thread adds
+// its pairs' contributions before the warp reduction, so one reduction serves
+// 2 NP pixels per lane.
 // kB entries are staged per batch (RasterConfig::backward_batch: 64, 128 or
 // 256 with two pixels per thread; 128 with four, where fewer threads share a
 // batch); `schedule` maps CTAs to tiles (for_each_tile).
